@@ -1,0 +1,59 @@
+// CircuitUnitaryOperationB200.h -- drop-in backend for QuantumSimEvo's
+// ICircuitUnitaryOperation (QuantumSimEvo/ICircuitUnitaryOperation.h:6-35),
+// standing in for CircuitUnitaryOperationGPU (CircuitUnitaryOperationGPU.h:10-48).
+//
+// Compiled inside the reference tree: it includes the reference's own
+// interface header and forwards every call to the C ABI of libqse_b200.so
+// (include/qse_b200.h).  Mirror protocol as the reference GPU backend
+// (CircuitUnitaryOperationGPU.cu:158-192): the device copy is authoritative
+// after any apply*, flush() copies it into the bound StateVector, and
+// markHostDirty() forces a re-upload before the next gate.  Errors throw
+// std::runtime_error instead of aborting the process.
+#ifndef CIRCUIT_UNITARY_OPERATION_B200_H
+#define CIRCUIT_UNITARY_OPERATION_B200_H
+
+#include <cstddef>
+#include <vector>
+
+#include "ICircuitUnitaryOperation.h"
+#include "Structurs.h"
+#include "qse_b200.h"
+
+class CircuitUnitaryOperationB200 : public ICircuitUnitaryOperation {
+public:
+    explicit CircuitUnitaryOperationB200(int device = 0);
+    ~CircuitUnitaryOperationB200() override;
+
+    void applyGate(StateVector& sv, const Gate2x2& gate, size_t q) override;
+    void applyCNOT(StateVector& sv, size_t control, size_t target) override;
+    void applyPauliX(StateVector& sv, size_t q) override;
+    void applyPauliY(StateVector& sv, size_t q) override;
+    void applyPauliZ(StateVector& sv, size_t q) override;
+    void applyPhase(StateVector& sv, size_t q, double theta) override;
+    void applyRotateX(StateVector& sv, size_t q, double theta) override;
+    void applyRotateY(StateVector& sv, size_t q, double theta) override;
+    void applyRotateZ(StateVector& sv, size_t q, double theta) override;
+    void applyHadamard(StateVector& sv, size_t targetQubit) override;
+    void applyCPhase(StateVector& sv, size_t control, size_t target, double theta) override;
+    void applyMCPhase(StateVector& sv, const std::vector<size_t>& controls, size_t target, double theta) override;
+    void applySwap(StateVector& sv, size_t q0, size_t q1) override;
+
+    void flush() override;
+    void markHostDirty() override;
+
+    // Extension used by a Circuit::execute that hands over its whole queue
+    // (the fusion planner path): one call, any number of passes.
+    void executeProgram(StateVector& sv, const std::vector<GateCommand>& commands);
+
+private:
+    void ensureOnDevice(StateVector& sv);
+    void check(int status, const char* what) const;
+    void timed(const char* label, int status);
+
+    qse_ctx* ctx_;
+    qse_state* state_;
+    StateVector* bound_;
+    bool hostDirty_;
+};
+
+#endif

@@ -1,0 +1,499 @@
+// engine.cu -- Circuit::execute (Circuit.cpp:64-120) on the device: gate
+// list -> planner -> one tile-kernel launch per pass; noise decisions and the
+// end-of-execute Pauli frame; expectation values and the adjoint sweep.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "planner.h"
+#include "qse_internal.h"
+#include "tile.cuh"
+
+namespace qse {
+
+double bound_angle(const qse_op& op, const double* params, size_t nparams)
+{
+    if (op.param < 0) return op.theta;
+    if (!params || size_t(op.param) >= nparams) fail(QSE_ERR_INVALID, "op parameter index out of range");
+    return op.theta + op.coeff * params[op.param];
+}
+
+uint64_t logical_to_physical_index(const qse_state* st, uint64_t L)
+{
+    uint64_t P = 0;
+    for (uint32_t q = 0; q < st->n; ++q) P |= ((L >> q) & 1) << st->perm[q];
+    return P;
+}
+
+uint64_t physical_to_logical_index(const qse_state* st, uint64_t P)
+{
+    uint64_t L = 0;
+    for (uint32_t q = 0; q < st->n; ++q) L |= ((P >> st->perm[q]) & 1) << q;
+    return L;
+}
+
+namespace {
+
+plan::Gate to_gate(const qse_op& op, double theta)
+{
+    plan::Gate g;
+    g.type = op.type;
+    g.t = op.target;
+    g.c = op.control;
+    g.cmask = op.controls;
+    g.theta = theta;
+    for (int i = 0; i < 8; ++i) g.m[i] = op.m[i];
+    return g;
+}
+
+void check_qubits(const plan::Gate& g, uint32_t n)
+{
+    auto bad = [&](uint32_t q) { return q >= n; };
+    switch (g.type) {
+    case QSE_GATE_IDENTITY: return;
+    case QSE_GATE_CNOT: case QSE_GATE_CPHASE: case QSE_GATE_SWAP:
+        if (bad(g.t) || bad(g.c)) fail(QSE_ERR_QUBIT, "qubit index out of range");
+        return;
+    case QSE_GATE_MCPHASE:
+        if (bad(g.t) || (n < 64 && (g.cmask >> n) != 0)) fail(QSE_ERR_QUBIT, "qubit index out of range");
+        return;
+    case QSE_GATE_H: case QSE_GATE_X: case QSE_GATE_Y: case QSE_GATE_Z: case QSE_GATE_PHASE:
+    case QSE_GATE_RX: case QSE_GATE_RY: case QSE_GATE_RZ: case QSE_GATE_2X2:
+        if (bad(g.t)) fail(QSE_ERR_QUBIT, "qubit index out of range");
+        return;
+    default: fail(QSE_ERR_UNSUPPORTED, "gate type " + std::to_string(g.type) + " is not executable");
+    }
+}
+
+// One kernel per gate, in program order, on physical qubits (perm[logical]).
+void apply_plain(qse_state* st, const plan::Gate& g)
+{
+    const uint32_t* P = st->perm;
+    switch (g.type) {
+    case QSE_GATE_IDENTITY: return;
+    case QSE_GATE_H: launch_h(st, P[g.t]); return;
+    case QSE_GATE_X: launch_x(st, P[g.t]); return;
+    case QSE_GATE_Y: launch_y(st, P[g.t]); return;
+    case QSE_GATE_Z: launch_z(st, P[g.t]); return;
+    case QSE_GATE_PHASE: launch_phase_mask(st, uint64_t(1) << P[g.t], std::cos(g.theta), std::sin(g.theta)); return;
+    case QSE_GATE_RX: launch_rx(st, P[g.t], std::cos(g.theta / 2.0), std::sin(g.theta / 2.0)); return;
+    case QSE_GATE_RY: launch_ry(st, P[g.t], std::cos(g.theta / 2.0), std::sin(g.theta / 2.0)); return;
+    case QSE_GATE_RZ:
+        launch_rz(st, P[g.t], std::cos(-g.theta / 2.0), std::sin(-g.theta / 2.0), std::cos(g.theta / 2.0),
+                  std::sin(g.theta / 2.0));
+        return;
+    case QSE_GATE_CNOT:
+        if (g.c == g.t) return;
+        launch_cnot(st, P[g.c], P[g.t]);
+        return;
+    case QSE_GATE_CPHASE:
+        launch_phase_mask(st, (uint64_t(1) << P[g.c]) | (uint64_t(1) << P[g.t]), std::cos(g.theta), std::sin(g.theta));
+        return;
+    case QSE_GATE_MCPHASE: {
+        uint64_t m = uint64_t(1) << P[g.t];
+        for (uint64_t s = g.cmask; s; s &= s - 1) m |= uint64_t(1) << P[__builtin_ctzll(s)];
+        launch_phase_mask(st, m, std::cos(g.theta), std::sin(g.theta));
+        return;
+    }
+    case QSE_GATE_SWAP:
+        if (g.t == g.c) return;
+        launch_swap(st, P[g.t], P[g.c]);
+        return;
+    case QSE_GATE_2X2: launch_gate2x2(st, P[g.t], g.m, 0); return;
+    default: fail(QSE_ERR_UNSUPPORTED, "gate type not executable");
+    }
+}
+
+size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+struct Uploaded {
+    std::vector<tile::PassArgs> args;
+};
+
+// Packs every pass program into one pinned buffer and one H2D copy.
+Uploaded upload_plan(qse_ctx* ctx, const plan::Plan& pl)
+{
+    std::vector<size_t> off(pl.passes.size() * 5);
+    size_t total = 0;
+    for (size_t i = 0; i < pl.passes.size(); ++i) {
+        const plan::PassProgram& p = pl.passes[i];
+        off[5 * i + 0] = total; total = align16(total + p.ops.size() * sizeof(plan::KOp));
+        off[5 * i + 1] = total; total = align16(total + p.layouts.size() * sizeof(plan::LayoutRec));
+        off[5 * i + 2] = total; total = align16(total + p.terms.size() * sizeof(plan::TermRec));
+        off[5 * i + 3] = total; total = align16(total + p.groups.size() * sizeof(plan::GroupRec));
+        off[5 * i + 4] = total; total = align16(total + p.mats.size() * sizeof(double));
+    }
+    total = std::max<size_t>(total, 16);
+    QSE_CUDA(cudaEventSynchronize(ctx->plan_event));
+    ctx->plan_host.reserve(total);
+    ctx->plan_buf.reserve(total);
+    char* h = static_cast<char*>(ctx->plan_host.ptr);
+    for (size_t i = 0; i < pl.passes.size(); ++i) {
+        const plan::PassProgram& p = pl.passes[i];
+        std::memcpy(h + off[5 * i + 0], p.ops.data(), p.ops.size() * sizeof(plan::KOp));
+        std::memcpy(h + off[5 * i + 1], p.layouts.data(), p.layouts.size() * sizeof(plan::LayoutRec));
+        std::memcpy(h + off[5 * i + 2], p.terms.data(), p.terms.size() * sizeof(plan::TermRec));
+        std::memcpy(h + off[5 * i + 3], p.groups.data(), p.groups.size() * sizeof(plan::GroupRec));
+        std::memcpy(h + off[5 * i + 4], p.mats.data(), p.mats.size() * sizeof(double));
+    }
+    QSE_CUDA(cudaMemcpyAsync(ctx->plan_buf.ptr, h, total, cudaMemcpyHostToDevice, ctx->stream));
+    QSE_CUDA(cudaEventRecord(ctx->plan_event, ctx->stream));
+    char* d = static_cast<char*>(ctx->plan_buf.ptr);
+    Uploaded up;
+    for (size_t i = 0; i < pl.passes.size(); ++i) {
+        const plan::PassProgram& p = pl.passes[i];
+        tile::PassArgs a{};
+        a.ops = reinterpret_cast<const plan::KOp*>(d + off[5 * i + 0]);
+        a.layouts = reinterpret_cast<const plan::LayoutRec*>(d + off[5 * i + 1]);
+        a.terms = reinterpret_cast<const plan::TermRec*>(d + off[5 * i + 2]);
+        a.groups = reinterpret_cast<const plan::GroupRec*>(d + off[5 * i + 3]);
+        a.mats = reinterpret_cast<const double*>(d + off[5 * i + 4]);
+        a.outer_mask = p.outer_mask;
+        a.nops = uint32_t(p.ops.size());
+        a.ngroups = uint32_t(p.groups.size());
+        a.nslots = uint32_t(p.slot_src.size());
+        a.layout0 = p.layout0;
+        a.k = p.k;
+        std::memcpy(a.tile_phys, p.tile_phys, 16);
+        up.args.push_back(a);
+    }
+    return up;
+}
+
+uint32_t tile_qubits_for(const qse_ctx* ctx, uint32_t n, uint32_t rb, uint32_t kmax)
+{
+    uint32_t k = std::min<uint32_t>(std::max(ctx->tile_qubits, int(rb) + 1), kmax);
+    return std::min(k, n);
+}
+
+// noisy gates of the list in program order (types in the rate map)
+void run_noise(qse_state* st, qse_noise* nz, const qse_op* ops, size_t nops, const double* inj, size_t ninj,
+               qse_exec_stats* stats)
+{
+    qse_ctx* ctx = st->ctx;
+    std::vector<int32_t> types;
+    std::vector<uint32_t> targets;
+    for (size_t i = 0; i < nops; ++i) {
+        int t = ops[i].type;
+        if (t >= 0 && t < 16 && nz->cfg.rates[t] >= 0.0) {
+            types.push_back(t);
+            targets.push_back(ops[i].target);
+        }
+    }
+    const size_t ng = types.size();
+    if (stats) stats->noisy_gates = ng;
+    if (ng == 0) return;
+    std::vector<double> uni;
+    if (nz->cfg.rng_mode == QSE_RNG_MT19937) {
+        uni.resize(2 * ng);
+        for (size_t i = 0; i < 2 * ng; ++i) uni[i] = nz->dist(nz->gen);
+    } else if (nz->cfg.rng_mode == QSE_RNG_INJECTED) {
+        if (!inj || ninj < 2 * ng) fail(QSE_ERR_INVALID, "injected noise needs 2 uniforms per noisy gate");
+        uni.assign(inj, inj + 2 * ng);
+    }
+    size_t bytes = ng * 4 + ng * 4 + uni.size() * 8 + 64;
+    ctx->host_small2.reserve(bytes);
+    ctx->scratch.reserve(bytes);
+    char* h = static_cast<char*>(ctx->host_small2.ptr);
+    size_t o_t = 0, o_g = align16(ng * 4), o_u = align16(o_g + ng * 4);
+    std::memcpy(h + o_t, types.data(), ng * 4);
+    std::memcpy(h + o_g, targets.data(), ng * 4);
+    if (!uni.empty()) std::memcpy(h + o_u, uni.data(), uni.size() * 8);
+    char* d = static_cast<char*>(ctx->scratch.ptr);
+    QSE_CUDA(cudaMemcpyAsync(d, h, o_u + uni.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+    noise_decide(nz, reinterpret_cast<const int32_t*>(d + o_t), reinterpret_cast<const uint32_t*>(d + o_g), ng,
+                 uni.empty() ? nullptr : reinterpret_cast<const double*>(d + o_u));
+    QSE_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+}  // namespace
+
+void execute_program(qse_state* st, const qse_op* ops, size_t nops, const double* params, size_t nparams,
+                     qse_noise* noise, const double* inj, size_t ninj, qse_exec_stats* stats)
+{
+    qse_ctx* ctx = st->ctx;
+    const uint64_t launches0 = ctx->launches;
+    if (stats) *stats = qse_exec_stats{};
+    std::vector<plan::Gate> gates;
+    gates.reserve(nops);
+    for (size_t i = 0; i < nops; ++i) {
+        gates.push_back(to_gate(ops[i], bound_angle(ops[i], params, nparams)));
+        check_qubits(gates.back(), st->n);
+    }
+    if (noise && noise->cfg.enabled) {
+        if (noise->n != st->n) fail(QSE_ERR_INVALID, "noise object was created for a different qubit count");
+        run_noise(st, noise, ops, nops, inj, ninj, stats);
+    }
+    uint64_t passes = 0;
+    if (!ctx->fusion || st->n < 4) {
+        for (const plan::Gate& g : gates) apply_plain(st, g);
+        passes = gates.size();
+    } else {
+        plan::Options opt;
+        opt.rb = 4;
+        opt.k = tile_qubits_for(ctx, st->n, 4, 12);
+        opt.max_gates = uint32_t(std::max(0, ctx->max_gates_per_pass));
+        plan::Plan pl = plan::build(gates, st->n, st->perm, opt);
+        Uploaded up = upload_plan(ctx, pl);
+        for (tile::PassArgs& a : up.args) {
+            a.psi = reinterpret_cast<double2*>(st->amp);
+            tile::launch_pass(ctx, a, st->n, 4, 1);
+        }
+        for (uint32_t q = 0; q < st->n; ++q) st->perm[q] = pl.perm_final[q];
+        passes = pl.passes.size();
+    }
+    if (noise && noise->cfg.enabled) launch_pauli_frame(st, noise->d_counts);
+    if (stats) {
+        stats->gates = nops;
+        stats->passes = passes;
+        stats->kernels = ctx->launches - launches0;
+    }
+}
+
+void apply_single(qse_state* st, const qse_op& op)
+{
+    plan::Gate g = to_gate(op, op.theta);
+    check_qubits(g, st->n);
+    apply_plain(st, g);
+}
+
+void canonicalize(qse_state* st)
+{
+    // restore logical == physical with physical qubit swaps (each a half sweep)
+    for (uint32_t q = 0; q < st->n; ++q) {
+        if (st->perm[q] == q) continue;
+        // find the logical qubit r currently sitting on physical q
+        uint32_t r = q;
+        for (uint32_t s = 0; s < st->n; ++s)
+            if (st->perm[s] == q) r = s;
+        launch_swap(st, q, st->perm[q]);
+        std::swap(st->perm[q], st->perm[r]);
+    }
+}
+
+// ---------------------------------------------------------------- observables
+namespace {
+
+constexpr int kRB = 256;
+
+__device__ __forceinline__ double obs_value(uint64_t x, const uint64_t* z, const double* w, uint32_t nt, double c)
+{
+    double v = c;
+    for (uint32_t t = 0; t < nt; ++t) v += (__popcll(x & z[t]) & 1) ? -w[t] : w[t];
+    return v;
+}
+
+// partial[b] = sum O(x)|psi_x|^2 over the block's range; lam = O psi if lam != nullptr
+__global__ void __launch_bounds__(kRB) k_obs(const double2* __restrict__ psi, double2* __restrict__ lam, uint64_t size,
+                                             const uint64_t* __restrict__ z, const double* __restrict__ w, uint32_t nt,
+                                             double c, double* __restrict__ partial)
+{
+    __shared__ double sh[kRB / 32];
+    extern __shared__ uint64_t sz[];
+    double* sw = reinterpret_cast<double*>(sz + nt);
+    for (uint32_t t = threadIdx.x; t < nt; t += blockDim.x) { sz[t] = z[t]; sw[t] = w[t]; }
+    __syncthreads();
+    double acc = 0.0;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < size; i += uint64_t(gridDim.x) * blockDim.x) {
+        double2 v = psi[i];
+        double o = obs_value(i, sz, sw, nt, c);
+        acc += o * (v.x * v.x + v.y * v.y);
+        if (lam) lam[i] = make_double2(o * v.x, o * v.y);
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int i = 0; i < kRB / 32; ++i) t += sh[i];
+        partial[blockIdx.x] = t;
+    }
+}
+
+// out[src[s]] = sum_b partial[s][b]
+__global__ void __launch_bounds__(kRB) k_reduce_slots(const double* __restrict__ partial, uint32_t nslots, uint64_t nb,
+                                                      const int32_t* __restrict__ src, double* __restrict__ out)
+{
+    __shared__ double sh[kRB / 32];
+    for (uint32_t s = blockIdx.x; s < nslots; s += gridDim.x) {
+        double acc = 0.0;
+        for (uint64_t b = threadIdx.x; b < nb; b += blockDim.x) acc += partial[uint64_t(s) * nb + b];
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (int i = 0; i < kRB / 32; ++i) t += sh[i];
+            out[src[s]] += t;
+        }
+        __syncthreads();
+    }
+}
+
+struct ObsDev {
+    const uint64_t* z;
+    const double* w;
+    uint32_t nt;
+    double c;
+};
+
+// Physical-qubit copy of the observable in device scratch (after `reserve_extra` bytes).
+ObsDev upload_obs(qse_state* st, const qse_observable* obs, char* dbase, char* hbase)
+{
+    ObsDev o{};
+    o.nt = uint32_t(obs->nterms);
+    o.c = obs->constant;
+    uint64_t* hz = reinterpret_cast<uint64_t*>(hbase);
+    double* hw = reinterpret_cast<double*>(hbase + 8 * obs->nterms);
+    for (size_t t = 0; t < obs->nterms; ++t) {
+        uint64_t m = obs->zmask[t], pm = 0;
+        if (st->n < 64 && (m >> st->n) != 0) fail(QSE_ERR_QUBIT, "observable acts on a qubit out of range");
+        for (; m; m &= m - 1) pm |= uint64_t(1) << st->perm[__builtin_ctzll(m)];
+        hz[t] = pm;
+        hw[t] = obs->weight[t];
+    }
+    QSE_CUDA(cudaMemcpyAsync(dbase, hbase, 16 * obs->nterms, cudaMemcpyHostToDevice, st->ctx->stream));
+    o.z = reinterpret_cast<const uint64_t*>(dbase);
+    o.w = reinterpret_cast<const double*>(dbase + 8 * obs->nterms);
+    return o;
+}
+
+double run_obs(qse_state* st, const qse_observable* obs, double2* lam)
+{
+    qse_ctx* ctx = st->ctx;
+    if (obs->nterms > 4096) fail(QSE_ERR_SIZE, "observable has too many terms");
+    const uint64_t size = st->size();
+    const unsigned grid = unsigned(std::min<uint64_t>((size + kRB - 1) / kRB, uint64_t(ctx->num_sms) * 8));
+    size_t obytes = align16(16 * obs->nterms);
+    ctx->scratch.reserve(obytes + size_t(grid) * 8 + 16);
+    ctx->host_small.reserve(obytes + size_t(grid) * 8 + 16);
+    QSE_CUDA(cudaStreamSynchronize(ctx->stream));  // host_small may still feed an earlier copy
+    char* d = static_cast<char*>(ctx->scratch.ptr);
+    char* h = static_cast<char*>(ctx->host_small.ptr);
+    ObsDev o = upload_obs(st, obs, d, h);
+    double* partial = reinterpret_cast<double*>(d + obytes);
+    k_obs<<<grid, kRB, 16 * obs->nterms, ctx->stream>>>(reinterpret_cast<const double2*>(st->amp), lam, size, o.z, o.w,
+                                                        o.nt, o.c, partial);
+    QSE_CUDA(cudaGetLastError());
+    count_launch(ctx);
+    double* hp = reinterpret_cast<double*>(h + obytes);
+    QSE_CUDA(cudaMemcpyAsync(hp, partial, size_t(grid) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    QSE_CUDA(cudaStreamSynchronize(ctx->stream));
+    double acc = 0.0;
+    for (unsigned b = 0; b < grid; ++b) acc += hp[b];
+    return acc;
+}
+
+plan::Gate inverse_gate(const qse_op& op, double theta, int32_t grad)
+{
+    plan::Gate g = to_gate(op, theta);
+    switch (op.type) {
+    case QSE_GATE_PHASE: case QSE_GATE_RX: case QSE_GATE_RY: case QSE_GATE_RZ:
+    case QSE_GATE_CPHASE: case QSE_GATE_MCPHASE:
+        g.theta = -theta;
+        break;
+    case QSE_GATE_2X2:
+        g.m[0] = op.m[0]; g.m[1] = -op.m[1];
+        g.m[2] = op.m[4]; g.m[3] = -op.m[5];
+        g.m[4] = op.m[2]; g.m[5] = -op.m[3];
+        g.m[6] = op.m[6]; g.m[7] = -op.m[7];
+        break;
+    default: break;
+    }
+    g.grad = grad;
+    return g;
+}
+
+bool parameterised(int type)
+{
+    return type == QSE_GATE_RX || type == QSE_GATE_RY || type == QSE_GATE_RZ || type == QSE_GATE_PHASE ||
+           type == QSE_GATE_CPHASE || type == QSE_GATE_MCPHASE;
+}
+
+}  // namespace
+
+double expectation(qse_state* st, const qse_observable* obs) { return run_obs(st, obs, nullptr); }
+
+double adjoint(qse_state* st, const qse_op* ops, size_t nops, const double* params, size_t nparams,
+               const qse_observable* obs, double* grad)
+{
+    qse_ctx* ctx = st->ctx;
+    if (st->n < 3) fail(QSE_ERR_SIZE, "adjoint needs at least 3 qubits");
+    // forward from |0..0>
+    launch_init_zero_state(st);
+    for (uint32_t q = 0; q < st->n; ++q) st->perm[q] = q;
+    execute_program(st, ops, nops, params, nparams, nullptr, nullptr, 0, nullptr);
+    if (!st->aux) QSE_CUDA(cudaMalloc(&st->aux, st->size() * 16));
+    double value = run_obs(st, obs, reinterpret_cast<double2*>(st->aux));
+
+    // reverse sweep over the inverse gates, gradient slots on parameterised ones
+    std::vector<plan::Gate> rev;
+    rev.reserve(nops);
+    for (size_t i = nops; i-- > 0;) {
+        double th = bound_angle(ops[i], params, nparams);
+        int32_t gid = (ops[i].param >= 0 && parameterised(ops[i].type)) ? int32_t(i) : -1;
+        rev.push_back(inverse_gate(ops[i], th, gid));
+    }
+    plan::Options opt;
+    opt.rb = 3;
+    opt.k = tile_qubits_for(ctx, st->n, 3, 11);
+    opt.grads = true;
+    opt.max_terms = 512;
+    opt.max_gates = 256;
+    plan::Plan pl = plan::build(rev, st->n, st->perm, opt);
+    Uploaded up = upload_plan(ctx, pl);
+
+    // occurrence gradients accumulate in scratch2: [nops] | slot partials
+    size_t max_part = 0;
+    for (size_t i = 0; i < pl.passes.size(); ++i)
+        max_part = std::max(max_part, pl.passes[i].slot_src.size() * (size_t(1) << (st->n - pl.passes[i].k)));
+    size_t srcmax = 0;
+    for (auto& p : pl.passes) srcmax = std::max(srcmax, p.slot_src.size());
+    size_t b_occ = align16(nops * 8 + 8), b_part = align16(max_part * 8 + 8), b_src = align16(srcmax * 4 + 4);
+    ctx->scratch2.reserve(b_occ + b_part + b_src * pl.passes.size() + 16);
+    char* base = static_cast<char*>(ctx->scratch2.ptr);
+    double* occ = reinterpret_cast<double*>(base);
+    double* part = reinterpret_cast<double*>(base + b_occ);
+    char* srcbase = base + b_occ + b_part;
+    QSE_CUDA(cudaMemsetAsync(occ, 0, nops * 8 + 8, ctx->stream));
+    // slot -> occurrence maps, one upload
+    {
+        size_t hb = b_src * pl.passes.size() + 16;
+        ctx->host_small2.reserve(hb);
+        char* h = static_cast<char*>(ctx->host_small2.ptr);
+        for (size_t i = 0; i < pl.passes.size(); ++i)
+            std::memcpy(h + i * b_src, pl.passes[i].slot_src.data(), pl.passes[i].slot_src.size() * 4);
+        QSE_CUDA(cudaMemcpyAsync(srcbase, h, b_src * pl.passes.size(), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    for (size_t i = 0; i < up.args.size(); ++i) {
+        tile::PassArgs a = up.args[i];
+        a.psi = reinterpret_cast<double2*>(st->amp);
+        a.lam = reinterpret_cast<double2*>(st->aux);
+        a.slot_partial = part;
+        tile::launch_pass(ctx, a, st->n, 3, 2);
+        if (a.nslots) {
+            uint64_t nb = uint64_t(1) << (st->n - a.k);
+            unsigned g = std::min<unsigned>(a.nslots, unsigned(ctx->num_sms) * 4);
+            k_reduce_slots<<<g, kRB, 0, ctx->stream>>>(part, a.nslots, nb,
+                                                        reinterpret_cast<const int32_t*>(srcbase + i * b_src), occ);
+            QSE_CUDA(cudaGetLastError());
+            count_launch(ctx);
+        }
+    }
+    for (uint32_t q = 0; q < st->n; ++q) st->perm[q] = pl.perm_final[q];
+    std::vector<double> hocc(nops);
+    QSE_CUDA(cudaMemcpyAsync(hocc.data(), occ, nops * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    QSE_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (size_t p = 0; p < nparams; ++p) grad[p] = 0.0;
+    for (size_t i = 0; i < nops; ++i) {
+        if (ops[i].param < 0 || !parameterised(ops[i].type)) continue;
+        // slot sums: X/Y/Z generators give 2 Im<l|G|s> directly; phase-type G = -P gives -2 Im<l|P|s>
+        double f = (ops[i].type == QSE_GATE_PHASE || ops[i].type == QSE_GATE_CPHASE ||
+                    ops[i].type == QSE_GATE_MCPHASE) ? -2.0 : 1.0;
+        grad[ops[i].param] += ops[i].coeff * f * hocc[i];
+    }
+    return value;
+}
+
+}  // namespace qse

@@ -1,0 +1,408 @@
+// gates.cu -- one kernel per gate (the "plain method"), state management kernels.
+//
+// These are the kernels behind ICircuitUnitaryOperation's per-gate entry
+// points (ICircuitUnitaryOperation.h:19-31) when the caller drives the backend
+// gate by gate, and behind qse_execute when fusion is switched off.  Each is a
+// grid-stride loop over the amplitudes a gate touches, with 16-byte complex128
+// loads and stores; a pair kernel visits only the 2^(n-1) pairs, a diagonal
+// kernel only the amplitudes whose mask bits are all set (the reference
+// launches 2^n threads and lets most of them idle, CircuitUnitaryOperationGPU.cu:74-117).
+#include "qse_internal.h"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+namespace qse {
+namespace {
+
+constexpr int kBlock = 256;
+
+__device__ __forceinline__ uint64_t insert0(uint64_t i, uint32_t q)
+{
+    return ((i >> q) << (q + 1)) | (i & ((uint64_t(1) << q) - 1));
+}
+
+// insert a 1 bit at every set position of `mask` (ascending), expanding i
+__device__ __forceinline__ uint64_t insert_ones(uint64_t i, uint64_t mask)
+{
+    while (mask) {
+        uint32_t b = __ffsll((long long)mask) - 1;
+        mask &= mask - 1;
+        i = insert0(i, b) | (uint64_t(1) << b);
+    }
+    return i;
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+unsigned grid_for(const qse_ctx* ctx, uint64_t work)
+{
+    uint64_t blocks = (work + kBlock - 1) / kBlock;
+    uint64_t cap = uint64_t(ctx->num_sms) * 32;
+    if (blocks > cap) blocks = cap;
+    if (blocks == 0) blocks = 1;
+    return unsigned(blocks);
+}
+
+// ---- pair kernels: (a[i0], a[i1]) with i1 = i0 | 2^q ----
+struct FH {
+    __device__ void operator()(double2& v0, double2& v1) const
+    {
+        const double s = 0.7071067811865475244;
+        double2 a = v0, b = v1;
+        v0 = make_double2((a.x + b.x) * s, (a.y + b.y) * s);
+        v1 = make_double2((a.x - b.x) * s, (a.y - b.y) * s);
+    }
+};
+struct FX {
+    __device__ void operator()(double2& v0, double2& v1) const { double2 t = v0; v0 = v1; v1 = t; }
+};
+struct FY {  // (-i v1, i v0)
+    __device__ void operator()(double2& v0, double2& v1) const
+    {
+        double2 a = v0, b = v1;
+        v0 = make_double2(b.y, -b.x);
+        v1 = make_double2(-a.y, a.x);
+    }
+};
+struct FRX {  // [[c, -is], [-is, c]]
+    double c, s;
+    __device__ void operator()(double2& v0, double2& v1) const
+    {
+        double2 a = v0, b = v1;
+        v0 = make_double2(c * a.x + s * b.y, c * a.y - s * b.x);
+        v1 = make_double2(s * a.y + c * b.x, -s * a.x + c * b.y);
+    }
+};
+struct FRY {  // [[c, -s], [s, c]]
+    double c, s;
+    __device__ void operator()(double2& v0, double2& v1) const
+    {
+        double2 a = v0, b = v1;
+        v0 = make_double2(c * a.x - s * b.x, c * a.y - s * b.y);
+        v1 = make_double2(s * a.x + c * b.x, s * a.y + c * b.y);
+    }
+};
+struct FRZ {  // diag(p0, p1)
+    double2 p0, p1;
+    __device__ void operator()(double2& v0, double2& v1) const { v0 = cmul(v0, p0); v1 = cmul(v1, p1); }
+};
+struct F2x2 {
+    double2 g00, g01, g10, g11;
+    __device__ void operator()(double2& v0, double2& v1) const
+    {
+        double2 a = v0, b = v1;
+        double2 x = cmul(g00, a), y = cmul(g01, b);
+        double2 z = cmul(g10, a), w = cmul(g11, b);
+        v0 = make_double2(x.x + y.x, x.y + y.y);
+        v1 = make_double2(z.x + w.x, z.y + w.y);
+    }
+};
+
+template <class F>
+__global__ void __launch_bounds__(kBlock) k_pairs(double2* __restrict__ a, uint64_t npairs, uint32_t q, F f)
+{
+    const uint64_t step = uint64_t(1) << q;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < npairs;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        uint64_t i0 = insert0(i, q);
+        double2 v0 = a[i0], v1 = a[i0 | step];
+        f(v0, v1);
+        a[i0] = v0;
+        a[i0 | step] = v1;
+    }
+}
+
+// Pairs on target t restricted to control bit c = 1 (CNOT): 2^(n-2) pairs.
+template <class F>
+__global__ void __launch_bounds__(kBlock) k_cpairs(double2* __restrict__ a, uint64_t npairs, uint32_t c,
+                                                   uint32_t t, F f)
+{
+    const uint32_t lo = c < t ? c : t, hi = c < t ? t : c;
+    const uint64_t cm = uint64_t(1) << c, tm = uint64_t(1) << t;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < npairs;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        uint64_t i0 = insert0(insert0(i, lo), hi) | cm;
+        double2 v0 = a[i0], v1 = a[i0 | tm];
+        f(v0, v1);
+        a[i0] = v0;
+        a[i0 | tm] = v1;
+    }
+}
+
+// Multiply every amplitude whose `mask` bits are all 1 by (c, s).
+__global__ void __launch_bounds__(kBlock) k_phase_mask(double2* __restrict__ a, uint64_t count, uint64_t mask,
+                                                       double c, double s)
+{
+    const double2 ph = make_double2(c, s);
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < count;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        uint64_t idx = insert_ones(i, mask);
+        a[idx] = cmul(a[idx], ph);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_negate_mask(double2* __restrict__ a, uint64_t count, uint32_t q)
+{
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < count;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        uint64_t idx = insert0(i, q) | (uint64_t(1) << q);
+        double2 v = a[idx];
+        a[idx] = make_double2(-v.x, -v.y);
+    }
+}
+
+// Swap |..1_q0..0_q1..> <-> |..0_q0..1_q1..>: 2^(n-2) pairs.
+__global__ void __launch_bounds__(kBlock) k_swap(double2* __restrict__ a, uint64_t count, uint32_t q0, uint32_t q1)
+{
+    const uint32_t lo = q0 < q1 ? q0 : q1, hi = q0 < q1 ? q1 : q0;
+    const uint64_t m0 = uint64_t(1) << q0, m1 = uint64_t(1) << q1;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < count;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        uint64_t base = insert0(insert0(i, lo), hi);
+        double2 x = a[base | m0], y = a[base | m1];
+        a[base | m0] = y;
+        a[base | m1] = x;
+    }
+}
+
+__global__ void k_set_first(double2* a) { a[0] = make_double2(1.0, 0.0); }
+
+__global__ void __launch_bounds__(kBlock) k_scale(double2* __restrict__ a, uint64_t count, double s)
+{
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < count;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        double2 v = a[i];
+        a[i] = make_double2(v.x * s, v.y * s);
+    }
+}
+
+// Noise::applyPauliNoise (Noise.cpp:34-44) as one pass: X on every qubit
+// with an odd bit-flip count, then Z on every qubit with an odd phase-flip
+// count.  Product of those operators: out[i] = (-1)^popc(i & z) * in[i ^ x].
+__global__ void k_pauli_masks(const int32_t* __restrict__ counts, uint32_t n, uint64_t* masks)
+{
+    uint64_t x = 0, z = 0;
+    for (uint32_t q = 0; q < n; ++q) {
+        if (counts[q] % 2 != 0) x |= uint64_t(1) << q;
+        if (counts[64 + q] % 2 != 0) z |= uint64_t(1) << q;
+    }
+    masks[0] = x;
+    masks[1] = z;
+}
+
+__global__ void __launch_bounds__(kBlock) k_pauli_frame(double2* __restrict__ a, uint64_t npairs,
+                                                        const uint64_t* __restrict__ masks, const uint32_t* perm)
+{
+    // masks are in logical qubits; map them to physical bits
+    __shared__ uint64_t sx, sz;
+    if (threadIdx.x == 0) {
+        uint64_t lx = masks[0], lz = masks[1], px = 0, pz = 0;
+        for (uint32_t q = 0; q < 64; ++q) {
+            if ((lx >> q) & 1) px |= uint64_t(1) << perm[q];
+            if ((lz >> q) & 1) pz |= uint64_t(1) << perm[q];
+        }
+        sx = px;
+        sz = pz;
+    }
+    __syncthreads();
+    const uint64_t x = sx, z = sz;
+    if (x == 0 && z == 0) return;
+    const uint32_t hb = x ? 63 - __clzll((long long)x) : 0;
+    for (uint64_t k = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; k < npairs;
+         k += uint64_t(gridDim.x) * blockDim.x) {
+        uint64_t i = insert0(k, hb);
+        uint64_t j = x ? (i ^ x) : (i | 1);
+        double2 vi = a[i], vj = a[j];
+        double si = (__popcll(i & z) & 1) ? -1.0 : 1.0;
+        double sj = (__popcll(j & z) & 1) ? -1.0 : 1.0;
+        if (x) {
+            a[i] = make_double2(si * vj.x, si * vj.y);
+            a[j] = make_double2(sj * vi.x, sj * vi.y);
+        } else {
+            a[i] = make_double2(si * vi.x, si * vi.y);
+            a[j] = make_double2(sj * vj.x, sj * vj.y);
+        }
+    }
+}
+
+// out[logical L] = amp[physical(L)] for L in [base, base + count)
+__global__ void __launch_bounds__(kBlock) k_gather_logical(const double2* __restrict__ a, double2* __restrict__ out,
+                                                           uint64_t base, uint64_t count, const uint32_t* perm,
+                                                           uint32_t n)
+{
+    __shared__ uint32_t sp[64];
+    if (threadIdx.x < 64) sp[threadIdx.x] = threadIdx.x < n ? perm[threadIdx.x] : 0;
+    __syncthreads();
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < count;
+         i += uint64_t(gridDim.x) * blockDim.x) {
+        uint64_t L = base + i, P = 0;
+        for (uint32_t q = 0; q < n; ++q) P |= ((L >> q) & 1) << sp[q];
+        out[i] = a[P];
+    }
+}
+
+template <class F>
+void launch_pairs(qse_state* st, uint32_t q, F f)
+{
+    uint64_t np = st->size() >> 1;
+    k_pairs<<<grid_for(st->ctx, np), kBlock, 0, st->ctx->stream>>>(reinterpret_cast<double2*>(st->amp), np, q, f);
+    QSE_CUDA(cudaGetLastError());
+    count_launch(st->ctx);
+}
+
+}  // namespace
+
+void launch_h(qse_state* st, uint32_t q) { launch_pairs(st, q, FH{}); }
+void launch_x(qse_state* st, uint32_t q) { launch_pairs(st, q, FX{}); }
+void launch_y(qse_state* st, uint32_t q) { launch_pairs(st, q, FY{}); }
+void launch_rx(qse_state* st, uint32_t q, double c, double s) { launch_pairs(st, q, FRX{c, s}); }
+void launch_ry(qse_state* st, uint32_t q, double c, double s) { launch_pairs(st, q, FRY{c, s}); }
+void launch_rz(qse_state* st, uint32_t q, double c0, double s0, double c1, double s1)
+{
+    launch_pairs(st, q, FRZ{make_double2(c0, s0), make_double2(c1, s1)});
+}
+
+void launch_gate2x2(qse_state* st, uint32_t q, const double m[8], uint64_t ctrl_mask)
+{
+    (void)ctrl_mask;
+    launch_pairs(st, q, F2x2{make_double2(m[0], m[1]), make_double2(m[2], m[3]), make_double2(m[4], m[5]),
+                             make_double2(m[6], m[7])});
+}
+
+void launch_z(qse_state* st, uint32_t q)
+{
+    uint64_t cnt = st->size() >> 1;
+    k_negate_mask<<<grid_for(st->ctx, cnt), kBlock, 0, st->ctx->stream>>>(reinterpret_cast<double2*>(st->amp), cnt, q);
+    QSE_CUDA(cudaGetLastError());
+    count_launch(st->ctx);
+}
+
+void launch_phase_mask(qse_state* st, uint64_t all_mask, double c, double s)
+{
+    uint64_t cnt = st->size() >> __builtin_popcountll(all_mask);
+    k_phase_mask<<<grid_for(st->ctx, cnt), kBlock, 0, st->ctx->stream>>>(reinterpret_cast<double2*>(st->amp), cnt,
+                                                                        all_mask, c, s);
+    QSE_CUDA(cudaGetLastError());
+    count_launch(st->ctx);
+}
+
+void launch_cphase(qse_state* st, uint32_t c, uint32_t t, double co, double si)
+{
+    launch_phase_mask(st, (uint64_t(1) << c) | (uint64_t(1) << t), co, si);
+}
+
+void launch_cnot(qse_state* st, uint32_t c, uint32_t t)
+{
+    uint64_t np = st->size() >> 2;
+    k_cpairs<<<grid_for(st->ctx, np), kBlock, 0, st->ctx->stream>>>(reinterpret_cast<double2*>(st->amp), np, c, t,
+                                                                   FX{});
+    QSE_CUDA(cudaGetLastError());
+    count_launch(st->ctx);
+}
+
+void launch_swap(qse_state* st, uint32_t q0, uint32_t q1)
+{
+    uint64_t cnt = st->size() >> 2;
+    k_swap<<<grid_for(st->ctx, cnt), kBlock, 0, st->ctx->stream>>>(reinterpret_cast<double2*>(st->amp), cnt, q0, q1);
+    QSE_CUDA(cudaGetLastError());
+    count_launch(st->ctx);
+}
+
+void launch_init_zero_state(qse_state* st)
+{
+    QSE_CUDA(cudaMemsetAsync(st->amp, 0, st->size() * 16, st->ctx->stream));
+    k_set_first<<<1, 1, 0, st->ctx->stream>>>(reinterpret_cast<double2*>(st->amp));
+    QSE_CUDA(cudaGetLastError());
+    count_launch(st->ctx);
+}
+
+void scale_state(qse_state* st, double s)
+{
+    uint64_t cnt = st->size();
+    k_scale<<<grid_for(st->ctx, cnt), kBlock, 0, st->ctx->stream>>>(reinterpret_cast<double2*>(st->amp), cnt, s);
+    QSE_CUDA(cudaGetLastError());
+    count_launch(st->ctx);
+}
+
+void launch_pauli_frame(qse_state* st, const int32_t* d_counts)
+{
+    qse_ctx* ctx = st->ctx;
+    ctx->scratch.reserve(64 * sizeof(uint32_t) + 2 * sizeof(uint64_t));
+    uint64_t* d_masks = static_cast<uint64_t*>(ctx->scratch.ptr);
+    uint32_t* d_perm = reinterpret_cast<uint32_t*>(d_masks + 2);
+    uint32_t perm[64];
+    for (uint32_t q = 0; q < 64; ++q) perm[q] = q < st->n ? st->perm[q] : 0;
+    ctx->host_small.reserve(sizeof(perm));
+    std::memcpy(ctx->host_small.ptr, perm, sizeof(perm));
+    QSE_CUDA(cudaMemcpyAsync(d_perm, ctx->host_small.ptr, sizeof(perm), cudaMemcpyHostToDevice, ctx->stream));
+    k_pauli_masks<<<1, 1, 0, ctx->stream>>>(d_counts, st->n, d_masks);
+    QSE_CUDA(cudaGetLastError());
+    uint64_t np = st->size() >> 1;
+    k_pauli_frame<<<grid_for(ctx, np), kBlock, 0, ctx->stream>>>(reinterpret_cast<double2*>(st->amp), np, d_masks,
+                                                                d_perm);
+    QSE_CUDA(cudaGetLastError());
+    count_launch(ctx, 2);
+    // the host buffer is reused by the next call only after this stream work
+    QSE_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+// flush(): device -> host in logical qubit order, logical indices
+// [first, first + count).  With the identity map a plain copy; otherwise
+// gathered chunk by chunk through device scratch.
+void download_range(qse_state* st, uint64_t first, uint64_t count, double* host)
+{
+    qse_ctx* ctx = st->ctx;
+    if (count == 0) return;
+    if (st->identity_perm()) {
+        QSE_CUDA(cudaMemcpyAsync(host, st->amp + 2 * first, count * 16, cudaMemcpyDeviceToHost, ctx->stream));
+        QSE_CUDA(cudaStreamSynchronize(ctx->stream));
+        return;
+    }
+    const uint64_t chunk = std::min<uint64_t>(count, uint64_t(1) << 24);
+    ctx->scratch.reserve(chunk * 16 + 64 * 4 + 256);
+    uint32_t perm[64] = {0};
+    for (uint32_t q = 0; q < st->n; ++q) perm[q] = st->perm[q];
+    char* d = static_cast<char*>(ctx->scratch.ptr);
+    uint32_t* d_perm = reinterpret_cast<uint32_t*>(d + chunk * 16);
+    ctx->host_small.reserve(sizeof(perm));
+    QSE_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(ctx->host_small.ptr, perm, sizeof(perm));
+    QSE_CUDA(cudaMemcpyAsync(d_perm, ctx->host_small.ptr, sizeof(perm), cudaMemcpyHostToDevice, ctx->stream));
+    for (uint64_t off = 0; off < count; off += chunk) {
+        uint64_t cnt = std::min(chunk, count - off);
+        k_gather_logical<<<grid_for(ctx, cnt), kBlock, 0, ctx->stream>>>(
+            reinterpret_cast<const double2*>(st->amp), reinterpret_cast<double2*>(d), first + off, cnt, d_perm, st->n);
+        QSE_CUDA(cudaGetLastError());
+        count_launch(ctx);
+        QSE_CUDA(cudaMemcpyAsync(host + 2 * off, d, cnt * 16, cudaMemcpyDeviceToHost, ctx->stream));
+        QSE_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+}
+
+void download_logical(qse_state* st, double* host) { download_range(st, 0, st->size(), host); }
+
+void permute_to_logical(qse_state* st, double* dst_device)
+{
+    qse_ctx* ctx = st->ctx;
+    ctx->scratch.reserve(64 * sizeof(uint32_t));
+    uint32_t perm[64] = {0};
+    for (uint32_t q = 0; q < st->n; ++q) perm[q] = st->perm[q];
+    ctx->host_small.reserve(sizeof(perm));
+    std::memcpy(ctx->host_small.ptr, perm, sizeof(perm));
+    QSE_CUDA(cudaMemcpyAsync(ctx->scratch.ptr, ctx->host_small.ptr, sizeof(perm), cudaMemcpyHostToDevice,
+                             ctx->stream));
+    uint64_t cnt = st->size();
+    k_gather_logical<<<grid_for(ctx, cnt), kBlock, 0, ctx->stream>>>(
+        reinterpret_cast<const double2*>(st->amp), reinterpret_cast<double2*>(dst_device), 0, cnt,
+        static_cast<const uint32_t*>(ctx->scratch.ptr), st->n);
+    QSE_CUDA(cudaGetLastError());
+    count_launch(ctx);
+    QSE_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+}  // namespace qse

@@ -1,0 +1,539 @@
+// planner.cpp -- gate-fusion planner and tile-program lowering.  Host only.
+//
+// Semantics preserved: gates are replayed as Circuit::execute does
+// (Circuit.cpp:64-120), in program order, except that a gate may run before
+// an earlier gate it commutes with.  Two gates commute here when, on every
+// qubit they share, both act diagonally (Z/PHASE/RZ/CPHASE/MCPHASE, and the
+// control of a CNOT).  SWAP (Circuit.cpp:59-62, applySwap) is a relabelling of
+// the logical->physical qubit map, applied with zero memory traffic.
+#include "planner.h"
+
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <sstream>
+#include <tuple>
+
+#include "qse_internal.h"
+
+namespace qse {
+namespace plan {
+namespace {
+
+constexpr double kInvSqrt2 = 0.7071067811865475244;  // CircuitUnitaryOperation.cpp:87
+
+enum Cls { C_DROP, C_N1, C_CX, C_DIAG, C_SWAP };
+
+struct Info {
+    Cls cls = C_DROP;
+    uint64_t nset = 0;  // logical qubits acted on non-diagonally
+    uint64_t dset = 0;  // logical qubits acted on diagonally (incl. controls)
+};
+
+inline uint64_t bit(uint32_t q) { return uint64_t(1) << q; }
+
+Info classify(const Gate& g, uint32_t n)
+{
+    auto chk = [&](uint32_t q) {
+        if (q >= n) fail(QSE_ERR_QUBIT, "qubit index " + std::to_string(q) + " out of range for " +
+                                            std::to_string(n) + " qubits");
+    };
+    Info r;
+    switch (g.type) {
+    case QSE_GATE_IDENTITY: return r;
+    case QSE_GATE_H: case QSE_GATE_X: case QSE_GATE_Y: case QSE_GATE_RX: case QSE_GATE_RY: case QSE_GATE_2X2:
+        chk(g.t);
+        r.cls = C_N1;
+        r.nset = bit(g.t);
+        return r;
+    case QSE_GATE_CNOT:
+        chk(g.t);
+        chk(g.c);
+        // control == target: the reference's condition (i & c) && (i < (i ^ t)) is never true
+        // (CircuitUnitaryOperation.cpp:47-51): a no-op.
+        if (g.c == g.t) return r;
+        r.cls = C_CX;
+        r.nset = bit(g.t);
+        r.dset = bit(g.c);
+        return r;
+    case QSE_GATE_Z: case QSE_GATE_PHASE: case QSE_GATE_RZ:
+        chk(g.t);
+        r.cls = C_DIAG;
+        r.dset = bit(g.t);
+        return r;
+    case QSE_GATE_CPHASE:
+        chk(g.t);
+        chk(g.c);
+        r.cls = C_DIAG;
+        r.dset = bit(g.t) | bit(g.c);
+        return r;
+    case QSE_GATE_MCPHASE:
+        chk(g.t);
+        if (n < 64 && (g.cmask >> n) != 0) fail(QSE_ERR_QUBIT, "mcphase control out of range");
+        r.cls = C_DIAG;
+        r.dset = bit(g.t) | g.cmask;
+        return r;
+    case QSE_GATE_SWAP:
+        chk(g.t);
+        chk(g.c);
+        if (g.t == g.c) return r;  // applySwap with q0 == q1 is a no-op (CircuitUnitaryOperationGPU.cu:338)
+        r.cls = C_SWAP;
+        r.nset = bit(g.t) | bit(g.c);
+        return r;
+    default:
+        fail(QSE_ERR_UNSUPPORTED, "gate type " + std::to_string(g.type) + " is not executable");
+    }
+}
+
+int popc(uint64_t x) { return __builtin_popcountll(x); }
+
+// One absorbed gate with its physical qubits resolved.
+struct Absorbed {
+    size_t src;
+    const Gate* g;
+    Cls cls;
+    uint32_t pt;     // physical target
+    uint32_t pc;     // physical control (CNOT)
+    uint64_t psup;   // physical support (diagonal)
+};
+
+// ---------- lowering of one pass ----------
+class Lowering {
+public:
+    Lowering(PassProgram& prog, uint32_t n, const Options& opt) : P(prog), n_(n), opt_(opt)
+    {
+        for (int i = 0; i < 64; ++i) loc_[i] = -1;
+        for (uint32_t b = 0; b < P.k; ++b) loc_[P.tile_phys[b]] = int(b);
+    }
+
+    void run(const std::vector<Absorbed>& abs, double gphase)
+    {
+        // tile-local bits needed in registers, in order
+        std::vector<int> need(abs.size(), -1);
+        for (size_t i = 0; i < abs.size(); ++i)
+            if (abs[i].cls == C_N1 || abs[i].cls == C_CX) need[i] = loc_[abs[i].pt];
+        need_ = &need;
+        choose_regs(0, nullptr);
+        P.layout0 = add_layout(nullptr);
+        double scale = 1.0;
+        for (size_t i = 0; i < abs.size(); ++i) {
+            const Absorbed& a = abs[i];
+            const Gate& g = *a.g;
+            if (a.cls == C_SWAP) continue;
+            if (a.cls == C_DIAG) {
+                if (opt_.grads && g.grad >= 0) emit_grad_diag(a);
+                add_diag_terms(a, gphase);
+                continue;
+            }
+            int tb = loc_[a.pt];
+            int p = reg_pos(tb);
+            if (p < 0) {
+                close_all(false, 1.0, 0.0);
+                std::vector<int> prev(reg_, reg_ + P.rb);
+                choose_regs(i, &prev);
+                KOp t{};
+                t.kind = K_TRANSPOSE;
+                t.g = uint16_t(add_layout(prev.data()));
+                P.ops.push_back(t);
+                p = reg_pos(tb);
+            }
+            close_reg(p);
+            if (opt_.grads && g.grad >= 0) emit_grad_pair(a, p);
+            KOp op{};
+            op.p = uint8_t(p);
+            if (a.cls == C_CX) {
+                op.kind = K_X;
+                set_control(op, a.pc);
+            } else {
+                switch (g.type) {
+                case QSE_GATE_H: op.kind = K_H; scale *= kInvSqrt2; break;
+                case QSE_GATE_X: op.kind = K_X; break;
+                case QSE_GATE_Y: op.kind = K_Y; break;
+                case QSE_GATE_RX: op.kind = K_RX; op.a = std::cos(g.theta / 2.0); op.b = std::sin(g.theta / 2.0); break;
+                case QSE_GATE_RY: op.kind = K_RY; op.a = std::cos(g.theta / 2.0); op.b = std::sin(g.theta / 2.0); break;
+                case QSE_GATE_2X2:
+                    op.kind = K_U;
+                    op.g = uint16_t(P.mats.size() / 8);
+                    P.mats.insert(P.mats.end(), g.m, g.m + 8);
+                    break;
+                default: fail(QSE_ERR_UNSUPPORTED, "internal: unexpected non-diagonal type");
+                }
+            }
+            P.ops.push_back(op);
+            P.n_nondiag++;
+        }
+        close_all(true, scale * std::cos(gphase_), scale * std::sin(gphase_));
+    }
+
+private:
+    PassProgram& P;
+    uint32_t n_;
+    const Options& opt_;
+    int loc_[64];
+    int reg_[4] = {0, 0, 0, 0};
+    int thr_[16];
+    int nthr_ = 0;
+    const std::vector<int>* need_ = nullptr;
+    double gphase_ = 0.0;
+
+    struct OG {
+        uint8_t kind, p, f;
+        uint16_t tcond;
+        std::vector<TermRec> terms;
+    };
+    std::map<std::tuple<int, int, int>, OG> open_;
+
+    int reg_pos(int tb) const
+    {
+        for (uint32_t i = 0; i < P.rb; ++i)
+            if (reg_[i] == tb) return int(i);
+        return -1;
+    }
+    int thr_pos(int tb) const
+    {
+        for (int i = 0; i < nthr_; ++i)
+            if (thr_[i] == tb) return i;
+        return -1;
+    }
+
+    // registers for the layout starting at gate index `from`: the next rb
+    // distinct needed bits, then bits of the previous layout, then high bits.
+    void choose_regs(size_t from, const std::vector<int>* prev)
+    {
+        std::vector<int> r;
+        auto has = [&](int b) { return std::find(r.begin(), r.end(), b) != r.end(); };
+        for (size_t i = from; i < need_->size() && r.size() < P.rb; ++i) {
+            int b = (*need_)[i];
+            if (b >= 0 && !has(b)) r.push_back(b);
+        }
+        if (prev)
+            for (int b : *prev)
+                if (r.size() < P.rb && !has(b)) r.push_back(b);
+        for (int b = int(P.k) - 1; b >= 0 && r.size() < P.rb; --b)
+            if (!has(b)) r.push_back(b);
+        std::sort(r.begin(), r.end());
+        for (uint32_t i = 0; i < P.rb; ++i) reg_[i] = r[i];
+        nthr_ = 0;
+        for (uint32_t b = 0; b < P.k; ++b)
+            if (reg_pos(int(b)) < 0) thr_[nthr_++] = int(b);
+    }
+
+    // Slot images for the shared-memory exchange from layout `prev` to the
+    // current one: L(e_b) = e_b ^ s_b (s_b in the low 3 bits, b >= 3), chosen so
+    // that the 8 lanes of each quarter-warp hit 8 distinct 16-byte bank groups
+    // both when writing (prev layout) and reading (new layout).
+    uint32_t add_layout(const int* prev)
+    {
+        LayoutRec rec{};
+        for (uint32_t i = 0; i < P.rb; ++i) rec.reg[i] = uint8_t(reg_[i]);
+        rec.nthr = uint8_t(nthr_);
+        uint32_t s[16] = {0};
+        if (prev && nthr_ >= 3) {
+            int pl[3], nl[3], np = 0;
+            for (uint32_t b = 0; b < P.k && np < 3; ++b) {
+                bool in_prev = false;
+                for (uint32_t i = 0; i < P.rb; ++i) in_prev |= prev[i] == int(b);
+                if (!in_prev) pl[np++] = int(b);
+            }
+            for (int i = 0; i < 3; ++i) nl[i] = thr_[i];
+            auto low3 = [&](int b, const uint32_t* sv) -> uint32_t { return b < 3 ? (1u << b) : sv[b]; };
+            auto rank_ok = [&](const int* lb, const uint32_t* sv) {
+                uint32_t v0 = low3(lb[0], sv), v1 = low3(lb[1], sv), v2 = low3(lb[2], sv);
+                if (!v0 || !v1 || !v2 || v0 == v1 || v0 == v2 || v1 == v2) return false;
+                return (v0 ^ v1) != v2;
+            };
+            uint64_t rng = 0x9E3779B97F4A7C15ull ^ (uint64_t(P.layouts.size()) * 0xBF58476D1CE4E5B9ull);
+            bool found = false;
+            for (int attempt = 0; attempt < 4096 && !found; ++attempt) {
+                uint32_t sv[16] = {0};
+                if (attempt > 0)
+                    for (uint32_t b = 3; b < P.k; ++b) {
+                        rng ^= rng << 13; rng ^= rng >> 7; rng ^= rng << 17;
+                        sv[b] = uint32_t(rng >> 61);
+                    }
+                if (rank_ok(pl, sv) && rank_ok(nl, sv)) {
+                    std::copy(sv, sv + 16, s);
+                    found = true;
+                }
+            }
+        }
+        for (uint32_t b = 0; b < 16; ++b) rec.L[b] = uint16_t((1u << b) ^ (b >= 3 ? s[b] : 0u));
+        P.layouts.push_back(rec);
+        return uint32_t(P.layouts.size() - 1);
+    }
+
+    void set_control(KOp& op, uint32_t pc)
+    {
+        int tb = loc_[pc];
+        if (tb < 0) {
+            op.ocond = bit(pc);
+            return;
+        }
+        int rp = reg_pos(tb);
+        if (rp >= 0) {
+            op.f = uint8_t(1u << rp);
+            return;
+        }
+        op.tcond = uint16_t(1u << thr_pos(tb));
+    }
+
+    // split a physical support into (register mask, thread mask, outer mask)
+    void split(uint64_t sup, uint8_t& f, uint16_t& tcond, uint64_t& ocond) const
+    {
+        f = 0;
+        tcond = 0;
+        ocond = 0;
+        for (uint64_t s = sup; s; s &= s - 1) {
+            uint32_t q = uint32_t(__builtin_ctzll(s));
+            int tb = loc_[q];
+            if (tb < 0) { ocond |= bit(q); continue; }
+            int rp = reg_pos(tb);
+            if (rp >= 0) f |= uint8_t(1u << rp);
+            else tcond |= uint16_t(1u << thr_pos(tb));
+        }
+    }
+
+    void add_term(uint64_t sup, double theta)
+    {
+        if (sup == 0) { gphase_ += theta; return; }
+        uint8_t f;
+        uint16_t tc;
+        uint64_t oc;
+        split(sup, f, tc, oc);
+        int nreg = popc(f);
+        int kind = nreg == 0 ? K_ACC_THR : (nreg == 1 ? K_ACC_REG : K_PHD);
+        int key2 = kind == K_ACC_REG ? __builtin_ctz(f) : (kind == K_PHD ? f : 0);
+        auto key = std::make_tuple(kind, key2, int(tc));
+        auto it = open_.find(key);
+        if (it == open_.end()) {
+            OG og{uint8_t(kind), uint8_t(kind == K_ACC_REG ? __builtin_ctz(f) : 0), f, tc, {}};
+            it = open_.emplace(key, std::move(og)).first;
+        }
+        it->second.terms.push_back(TermRec{oc, theta});
+    }
+
+    void add_diag_terms(const Absorbed& a, double& /*unused*/)
+    {
+        const Gate& g = *a.g;
+        switch (g.type) {
+        case QSE_GATE_Z: add_term(a.psup, M_PI); break;
+        case QSE_GATE_PHASE: case QSE_GATE_CPHASE: case QSE_GATE_MCPHASE: add_term(a.psup, g.theta); break;
+        case QSE_GATE_RZ:  // diag(e^{-it/2}, e^{it/2}) = e^{-it/2} diag(1, e^{it})
+            add_term(a.psup, g.theta);
+            gphase_ += -g.theta / 2.0;
+            break;
+        default: fail(QSE_ERR_UNSUPPORTED, "internal: unexpected diagonal type");
+        }
+    }
+
+    uint16_t emit_group(OG& og)
+    {
+        GroupRec gr{};
+        gr.first = uint32_t(P.terms.size());
+        gr.count = uint32_t(og.terms.size());
+        gr.direct = og.kind == K_PHD ? 1u : 0u;
+        P.terms.insert(P.terms.end(), og.terms.begin(), og.terms.end());
+        P.groups.push_back(gr);
+        return uint16_t(P.groups.size() - 1);
+    }
+
+    void close_reg(int p)
+    {
+        bool acc = false;
+        for (auto it = open_.begin(); it != open_.end();) {
+            OG& og = it->second;
+            bool hit = (og.kind == K_ACC_REG && og.p == p) || (og.kind == K_PHD && ((og.f >> p) & 1));
+            if (!hit) { ++it; continue; }
+            KOp op{};
+            op.kind = og.kind;
+            op.p = og.p;
+            op.f = og.f;
+            op.tcond = og.tcond;
+            op.g = emit_group(og);
+            P.ops.push_back(op);
+            acc |= og.kind == K_ACC_REG;
+            it = open_.erase(it);
+        }
+        if (acc) {
+            KOp fl{};
+            fl.kind = K_FLUSH_REG;
+            fl.p = uint8_t(p);
+            P.ops.push_back(fl);
+        }
+    }
+
+    void close_all(bool final, double ca, double cb)
+    {
+        uint8_t fmask = 0;
+        bool thr = false;
+        for (auto& kv : open_) {
+            OG& og = kv.second;
+            KOp op{};
+            op.kind = og.kind;
+            op.p = og.p;
+            op.f = og.f;
+            op.tcond = og.tcond;
+            op.g = emit_group(og);
+            P.ops.push_back(op);
+            if (og.kind == K_ACC_REG) fmask |= uint8_t(1u << og.p);
+            if (og.kind == K_ACC_THR) thr = true;
+        }
+        open_.clear();
+        if (final || fmask || thr) {
+            KOp fl{};
+            fl.kind = K_FLUSH_ALL;
+            fl.f = fmask;
+            fl.a = final ? ca : 1.0;
+            fl.b = final ? cb : 0.0;
+            P.ops.push_back(fl);
+        }
+    }
+
+    uint16_t new_slot(int32_t src)
+    {
+        P.slot_src.push_back(src);
+        return uint16_t(P.slot_src.size() - 1);
+    }
+
+    void emit_grad_pair(const Absorbed& a, int p)
+    {
+        const Gate& g = *a.g;
+        KOp op{};
+        op.p = uint8_t(p);
+        if (g.type == QSE_GATE_RX) op.kind = K_GRAD_X;
+        else if (g.type == QSE_GATE_RY) op.kind = K_GRAD_Y;
+        else return;
+        op.g = new_slot(g.grad);
+        P.ops.push_back(op);
+    }
+
+    void emit_grad_diag(const Absorbed& a)
+    {
+        const Gate& g = *a.g;
+        KOp op{};
+        if (g.type == QSE_GATE_RZ) {
+            op.kind = K_GRAD_Z;
+            uint8_t f;
+            split(a.psup, f, op.tcond, op.ocond);
+            op.p = f ? uint8_t(__builtin_ctz(f)) : uint8_t(255);
+        } else if (g.type == QSE_GATE_PHASE || g.type == QSE_GATE_CPHASE || g.type == QSE_GATE_MCPHASE) {
+            op.kind = K_GRAD_P;
+            split(a.psup, op.f, op.tcond, op.ocond);
+        } else {
+            return;
+        }
+        op.g = new_slot(g.grad);
+        P.ops.push_back(op);
+    }
+};
+
+}  // namespace
+
+Plan build(const std::vector<Gate>& gates, uint32_t n, const uint32_t* perm_in, const Options& opt)
+{
+    if (n == 0 || n > 40) fail(QSE_ERR_SIZE, "planner: unsupported qubit count");
+    Plan plan;
+    uint32_t perm[64];
+    for (uint32_t q = 0; q < 64; ++q) perm[q] = q < n ? perm_in[q] : q;
+    std::vector<Info> info(gates.size());
+    std::vector<size_t> remaining;
+    for (size_t i = 0; i < gates.size(); ++i) {
+        info[i] = classify(gates[i], n);
+        if (info[i].cls != C_DROP) remaining.push_back(i);
+    }
+    plan.gates = gates.size();
+    const uint32_t k = std::min<uint32_t>(opt.k, n);
+    const uint32_t seed_bits = std::min<uint32_t>(3, k);
+
+    while (!remaining.empty()) {
+        uint64_t T = 0;
+        for (uint32_t q = 0; q < seed_bits; ++q) T |= bit(q);
+        uint64_t bN = 0, bD = 0;
+        std::vector<Absorbed> abs;
+        std::vector<size_t> deferred;
+        uint32_t nN = 0, nterms = 0;
+        double gph = 0.0;
+        for (size_t idx : remaining) {
+            const Info& in = info[idx];
+            const Gate& g = gates[idx];
+            bool blocked = ((in.nset | in.dset) & bN) || (in.nset & bD);
+            if (!blocked) {
+                if (in.cls == C_SWAP) {
+                    std::swap(perm[g.t], perm[g.c]);
+                    abs.push_back(Absorbed{idx, &g, C_SWAP, 0, 0, 0});
+                    continue;
+                }
+                if (in.cls == C_DIAG) {
+                    if (nterms < opt.max_terms) {
+                        uint64_t ps = 0;
+                        for (uint64_t s = in.dset; s; s &= s - 1) ps |= bit(perm[__builtin_ctzll(s)]);
+                        abs.push_back(Absorbed{idx, &g, C_DIAG, perm[g.t], 0, ps});
+                        ++nterms;
+                        continue;
+                    }
+                } else {
+                    uint64_t pt = bit(perm[g.t]);
+                    bool fits = (T & pt) || uint32_t(popc(T)) < k;
+                    bool capped = opt.max_gates && nN >= opt.max_gates;
+                    if (fits && !capped) {
+                        T |= pt;
+                        abs.push_back(Absorbed{idx, &g, in.cls, perm[g.t], in.cls == C_CX ? perm[g.c] : 0, 0});
+                        ++nN;
+                        continue;
+                    }
+                }
+            }
+            deferred.push_back(idx);
+            bN |= in.nset;
+            bD |= in.dset;
+        }
+        // fill the tile with the lowest unused physical qubits
+        for (uint32_t q = 0; q < n && uint32_t(popc(T)) < k; ++q) T |= bit(q);
+        PassProgram prog;
+        prog.k = k;
+        prog.rb = opt.rb;
+        uint32_t b = 0;
+        for (uint32_t q = 0; q < n; ++q)
+            if ((T >> q) & 1) prog.tile_phys[b++] = uint8_t(q);
+        uint64_t all = n >= 64 ? ~uint64_t(0) : (bit(n) - 1);
+        prog.outer_mask = all & ~T;
+        prog.ngates = uint32_t(abs.size());
+        for (const Absorbed& a : abs) {
+            prog.order.push_back(uint32_t(a.src));
+            prog.phys_target.push_back(a.pt);
+        }
+        Lowering low(prog, n, opt);
+        low.run(abs, gph);
+        plan.passes.push_back(std::move(prog));
+        remaining.swap(deferred);
+    }
+    for (uint32_t q = 0; q < 64; ++q) plan.perm_final[q] = perm[q];
+    return plan;
+}
+
+std::string describe(const Plan& p)
+{
+    std::ostringstream os;
+    os << "{\"passes\":[";
+    for (size_t i = 0; i < p.passes.size(); ++i) {
+        const PassProgram& pp = p.passes[i];
+        if (i) os << ",";
+        os << "{\"k\":" << pp.k << ",\"tile\":[";
+        for (uint32_t b = 0; b < pp.k; ++b) os << (b ? "," : "") << int(pp.tile_phys[b]);
+        os << "],\"ops\":" << pp.ops.size() << ",\"groups\":" << pp.groups.size() << ",\"terms\":" << pp.terms.size()
+           << ",\"layouts\":" << pp.layouts.size() << ",\"gates\":" << pp.ngates
+           << ",\"nondiag\":" << pp.n_nondiag << ",\"order\":[";
+        for (size_t j = 0; j < pp.order.size(); ++j)
+            os << (j ? "," : "") << "[" << pp.order[j] << "," << pp.phys_target[j] << "]";
+        os << "],\"kinds\":[";
+        for (size_t j = 0; j < pp.ops.size(); ++j) os << (j ? "," : "") << int(pp.ops[j].kind);
+        os << "]}";
+    }
+    os << "],\"perm\":[";
+    for (uint32_t q = 0; q < 64; ++q) os << (q ? "," : "") << p.perm_final[q];
+    os << "]}";
+    return os.str();
+}
+
+}  // namespace plan
+}  // namespace qse

@@ -1,0 +1,140 @@
+// qse_internal.h -- host-side structures shared by the CUDA and C++ sources of
+// libqse_b200.so.  Not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/qse_b200.h"
+
+namespace qse {
+
+// Exception carrying a C-ABI status; caught at the extern "C" boundary.
+struct Error : std::runtime_error {
+    int status;
+    Error(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+[[noreturn]] void fail(int status, const std::string& msg);
+void cuda_check(cudaError_t e, const char* what, const char* file, int line);
+#define QSE_CUDA(call) ::qse::cuda_check((call), #call, __FILE__, __LINE__)
+
+// Growable device buffer owned by a context.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    void reserve(size_t n);
+    void release();
+    ~DevBuf() { release(); }
+};
+
+// Pinned host staging buffer.
+struct HostBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    void reserve(size_t n);
+    void release();
+    ~HostBuf() { release(); }
+};
+
+}  // namespace qse
+
+struct qse_ctx {
+    int device = 0;
+    int num_sms = 148;
+    size_t smem_optin = 0;
+    cudaStream_t stream = nullptr;
+    // planner knobs
+    int fusion = 1;
+    int tile_qubits = 12;
+    int max_gates_per_pass = 0;
+    int sample_mode = 0;
+    uint64_t launches = 0;
+    // scratch shared by the calls on this context (single host thread, like the reference backend)
+    qse::DevBuf plan_buf;    // uploaded pass programs
+    qse::HostBuf plan_host;  // pinned staging for the pass programs
+    qse::DevBuf scratch;     // reductions, sampling, noise decisions
+    qse::DevBuf scratch2;
+    qse::HostBuf host_small; // pinned small results
+    qse::HostBuf host_small2;
+    cudaEvent_t plan_event = nullptr;  // last H2D copy out of plan_host
+};
+
+struct qse_state {
+    qse_ctx* ctx = nullptr;
+    uint32_t n = 0;
+    double* amp = nullptr;       // 2^n complex128 (interleaved), physical qubit order
+    double* aux = nullptr;       // second state (adjoint |lambda>), allocated on first use
+    uint32_t perm[64];           // logical qubit -> physical bit
+    bool identity_perm() const {
+        for (uint32_t q = 0; q < n; ++q)
+            if (perm[q] != q) return false;
+        return true;
+    }
+    size_t size() const { return size_t(1) << n; }
+};
+
+struct qse_noise {
+    qse_ctx* ctx = nullptr;
+    uint32_t n = 0;
+    qse_noise_config cfg{};
+    uint64_t draws = 0;          // noisy gates so far (Philox counter)
+    int32_t* d_counts = nullptr; // device: bit[64], phase[64], then rates double[16]
+    // QSE_RNG_MT19937: the generator and distribution of Noise.cpp:7-8
+    std::mt19937 gen;
+    std::uniform_real_distribution<double> dist{0.0, 1.0};
+};
+
+namespace qse {
+
+// Launch bookkeeping.
+inline void count_launch(qse_ctx* ctx, uint64_t n = 1) { ctx->launches += n; }
+
+// ---- per-gate ("plain method") kernels: gates.cu ----
+void launch_gate2x2(qse_state* st, uint32_t q, const double m[8], uint64_t ctrl_mask);
+void launch_h(qse_state* st, uint32_t q);
+void launch_x(qse_state* st, uint32_t q);
+void launch_y(qse_state* st, uint32_t q);
+void launch_z(qse_state* st, uint32_t q);
+void launch_phase_mask(qse_state* st, uint64_t all_mask, double c, double s);  // phase/cphase/mcphase
+void launch_cphase(qse_state* st, uint32_t c, uint32_t t, double co, double si);
+void launch_rx(qse_state* st, uint32_t q, double c, double s);
+void launch_ry(qse_state* st, uint32_t q, double c, double s);
+void launch_rz(qse_state* st, uint32_t q, double c0, double s0, double c1, double s1);
+void launch_cnot(qse_state* st, uint32_t c, uint32_t t);
+void launch_swap(qse_state* st, uint32_t q0, uint32_t q1);
+void launch_init_zero_state(qse_state* st);
+void launch_pauli_frame(qse_state* st, const int32_t* d_counts);      // Noise::applyPauliNoise
+void permute_to_logical(qse_state* st, double* dst_device);           // gather into logical order
+void scale_state(qse_state* st, double s);
+
+// ---- fused execution (engine.cu / planner.cpp / tile.cu) ----
+void execute_program(qse_state* st, const qse_op* ops, size_t nops, const double* params, size_t nparams,
+                     qse_noise* noise, const double* inj, size_t ninj, qse_exec_stats* stats);
+void canonicalize(qse_state* st);
+
+// ---- sampling (sample.cu) ----
+void sample(qse_state* st, const double* u_host, size_t nshots, uint64_t seed, uint64_t* out_host);
+uint64_t measure(qse_state* st, double u);
+double total_probability(qse_state* st);
+
+// ---- noise (noise.cu) ----
+void noise_decide(qse_noise* nz, const int32_t* d_types, const uint32_t* d_targets, size_t ngates,
+                  const double* d_uniforms);
+// ---- observables / adjoint (adjoint.cu) ----
+double expectation(qse_state* st, const qse_observable* obs);
+double adjoint(qse_state* st, const qse_op* ops, size_t nops, const double* params, size_t nparams,
+               const qse_observable* obs, double* grad);
+
+// helpers
+uint64_t logical_to_physical_index(const qse_state* st, uint64_t logical);
+uint64_t physical_to_logical_index(const qse_state* st, uint64_t physical);
+double bound_angle(const qse_op& op, const double* params, size_t nparams);
+
+}  // namespace qse

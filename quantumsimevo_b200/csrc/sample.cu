@@ -1,0 +1,538 @@
+// sample.cu -- device StateVector::sample / measure (StateVector.cpp:77-156).
+//
+// The reference computes cum[i] = fl(cum[i-1] + p_i), p_i = fl(re^2 + im^2),
+// sequentially in index order, then answers each shot with the first i such
+// that cum[i] >= u * total (std::lower_bound).  A plain parallel scan rounds
+// differently, and at 30 qubits the sequential chain's own rounding (up to
+// ~1e-7 of the total) exceeds the probability of a typical basis state, so
+// the outcome index would differ for many shots.  This file reproduces the
+// sequential chain bit for bit with a parallel algorithm:
+//
+//   While the running sum c stays inside one binade [2^e, 2^(e+1)), every
+//   addition rounds to the fixed grid G = 2^(e-52), so with C = c/G an integer
+//   the step is C += round(p_i / G), where a tie (p_i/G exactly k + 1/2)
+//   rounds so that C stays even.  A step is therefore the map
+//   x -> x + d[x mod 2] (two offsets, one per parity of the incoming sum), and
+//   such maps compose associatively: a block of elements folds into one
+//   (d_even, d_odd) pair, and a block-wide scan gives every prefix.  When the
+//   sum leaves the binade (C reaches 2^53) that single step is redone with a
+//   real FP64 addition and the scan restarts on the new grid; c only grows, so
+//   there are at most a few dozen such restarts in the whole vector.
+//
+// Passes: (1) per-block approximate sums, (2) a scan of those to guess each
+// block's binade, (3) per-block (d_even, d_odd) on the guessed grid,
+// (4) one CTA walks the blocks in order with the exact running sum (blocks
+// whose guess fails are redone exactly), (5) every block writes its exact
+// cumulative values.  Shots then binary-search the block starts and the
+// block's values.
+#include <cuda_runtime.h>
+
+#include "philox.cuh"
+#include "qse_internal.h"
+
+namespace qse {
+namespace {
+
+constexpr int kBT = 256;            // threads per block
+constexpr int kEPT = 16;            // elements per thread
+constexpr int kBS = kBT * kEPT;     // elements per block (4096)
+constexpr uint64_t kTwo53 = uint64_t(1) << 53;
+
+struct Summ {                       // block fold on a guessed grid
+    uint64_t d0, d1;                // offsets for even / odd incoming sum
+    int32_t e;                      // grid exponent guessed (INT32_MIN: no guess)
+    int32_t ok;                     // 0: a step may leave the binade
+};
+
+__device__ __forceinline__ double norm2(double2 a)
+{
+    // std::norm(complex<double>) = re*re + im*im, two roundings, no FMA
+    return __dadd_rn(__dmul_rn(a.x, a.x), __dmul_rn(a.y, a.y));
+}
+
+struct PermMap {
+    uint32_t n;
+    uint32_t identity;
+    uint8_t p[64];
+};
+
+__device__ __forceinline__ uint64_t phys_index(uint64_t L, const PermMap& pm)
+{
+    if (pm.identity) return L;
+    uint64_t P = 0;
+    for (uint32_t q = 0; q < pm.n; ++q) P |= ((L >> q) & 1) << pm.p[q];
+    return P;
+}
+
+// epoch of a running sum: exponent of its binade (subnormals and 0 share -1022)
+__device__ __forceinline__ int epoch_of(double c)
+{
+    if (c < 2.2250738585072014e-308) return -1022;
+    return ilogb(c);
+}
+
+// element map x -> x + d[x&1] on grid 2^(e-52); returns false if p alone leaves the binade
+__device__ __forceinline__ bool elem_map(double p, int e, uint64_t& d0, uint64_t& d1)
+{
+    if (p >= ldexp(1.0, e + 1)) { d0 = d1 = kTwo53; return false; }
+    double q = ldexp(p, 52 - e);
+    double f = floor(q);
+    double fr = q - f;
+    uint64_t fi = uint64_t(f);
+    if (fr > 0.5) { d0 = d1 = fi + 1; }
+    else if (fr < 0.5) { d0 = d1 = fi; }
+    else if (fi & 1) { d0 = fi + 1; d1 = fi; }       // tie: result must be even
+    else { d0 = fi; d1 = fi + 1; }
+    return true;
+}
+
+__device__ __forceinline__ void compose(uint64_t a0, uint64_t a1, uint64_t b0, uint64_t b1, uint64_t& r0, uint64_t& r1)
+{
+    // first a, then b
+    r0 = a0 + ((a0 & 1) ? b1 : b0);
+    r1 = a1 + (((1 + a1) & 1) ? b1 : b0);
+}
+
+// block-wide inclusive scan of parity maps; returns the inclusive prefix of
+// this thread's last element and fills excl (exclusive prefix of the thread)
+__device__ void block_scan_maps(uint64_t t0, uint64_t t1, uint64_t& ex0, uint64_t& ex1, uint64_t* sh)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    uint64_t i0 = t0, i1 = t1;
+    // warp inclusive scan
+    for (int o = 1; o < 32; o <<= 1) {
+        uint64_t u0 = __shfl_up_sync(0xffffffffu, i0, o);
+        uint64_t u1 = __shfl_up_sync(0xffffffffu, i1, o);
+        if (lane >= o) {
+            uint64_t r0, r1;
+            compose(u0, u1, i0, i1, r0, r1);
+            i0 = r0;
+            i1 = r1;
+        }
+    }
+    if (lane == 31) { sh[2 * warp] = i0; sh[2 * warp + 1] = i1; }
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        uint64_t w0 = lane < nw ? sh[2 * lane] : 0, w1 = lane < nw ? sh[2 * lane + 1] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint64_t u0 = __shfl_up_sync(0xffffffffu, w0, o);
+            uint64_t u1 = __shfl_up_sync(0xffffffffu, w1, o);
+            if (lane >= o) {
+                uint64_t r0, r1;
+                compose(u0, u1, w0, w1, r0, r1);
+                w0 = r0;
+                w1 = r1;
+            }
+        }
+        if (lane < nw) { sh[64 + 2 * lane] = w0; sh[64 + 2 * lane + 1] = w1; }
+    }
+    __syncthreads();
+    // exclusive prefix for this thread = (warp prefix before this warp) then (lanes before)
+    uint64_t w0 = 0, w1 = 0;
+    if (warp > 0) { w0 = sh[64 + 2 * (warp - 1)]; w1 = sh[64 + 2 * (warp - 1) + 1]; }
+    uint64_t l0 = __shfl_up_sync(0xffffffffu, i0, 1), l1 = __shfl_up_sync(0xffffffffu, i1, 1);
+    if (lane == 0) { l0 = 0; l1 = 0; }
+    compose(w0, w1, l0, l1, ex0, ex1);
+    __syncthreads();
+}
+
+// Exact sequential cumulative sums of one block of `cnt` (<= kBS) values held
+// as p[0..kEPT) per thread (element index = tid*kEPT + j), starting from the
+// exact running sum c_in.  Writes the values to out (if non-null) and returns
+// the block's final sum.  Must be called by all threads of the block.
+__device__ double block_exact(const double (&p)[kEPT], uint32_t cnt, double c_in, double* out, uint64_t* sh)
+{
+    __shared__ double s_c;
+    __shared__ int s_t;
+    const uint32_t tid = threadIdx.x;
+    uint32_t pos = 0;
+    double c = c_in;
+    while (pos < cnt) {
+        const int e = epoch_of(c);
+        const double G = ldexp(1.0, e - 52);
+        const uint64_t C = uint64_t(ldexp(c, 52 - e));
+        // this thread's fold over its elements >= pos
+        uint64_t d[kEPT][2];
+        uint64_t t0 = 0, t1 = 0;
+        int bad = kBS;
+#pragma unroll
+        for (int j = 0; j < kEPT; ++j) {
+            uint32_t i = tid * kEPT + j;
+            uint64_t a0 = 0, a1 = 0;
+            if (i >= pos && i < cnt) {
+                if (!elem_map(p[j], e, a0, a1) && bad == kBS) bad = int(i);
+            }
+            d[j][0] = a0;
+            d[j][1] = a1;
+            uint64_t r0, r1;
+            compose(t0, t1, a0, a1, r0, r1);
+            t0 = r0;
+            t1 = r1;
+        }
+        uint64_t ex0, ex1;
+        block_scan_maps(t0, t1, ex0, ex1, sh);
+        // running values; first index that reaches 2^53 or is flagged
+        uint64_t run0 = ex0, run1 = ex1;
+        int first = bad;
+        uint64_t Ci[kEPT];
+#pragma unroll
+        for (int j = 0; j < kEPT; ++j) {
+            uint64_t r0, r1;
+            compose(run0, run1, d[j][0], d[j][1], r0, r1);
+            run0 = r0;
+            run1 = r1;
+            uint64_t v = C + ((C & 1) ? run1 : run0);
+            Ci[j] = v;
+            uint32_t i = tid * kEPT + j;
+            if (i >= pos && i < cnt && v >= kTwo53 && int(i) < first) first = int(i);
+        }
+        if (tid == 0) s_t = int(cnt);
+        __syncthreads();
+        if (first < int(cnt)) atomicMin(&s_t, first);
+        __syncthreads();
+        const uint32_t t = uint32_t(s_t);
+        // values before t are exact on this grid
+#pragma unroll
+        for (int j = 0; j < kEPT; ++j) {
+            uint32_t i = tid * kEPT + j;
+            if (i >= pos && i < t && out) out[i] = double(Ci[j]) * G;
+            if (t < cnt && i >= pos && i + 1 == t) s_c = double(Ci[j]) * G;   // c_{t-1}
+            if (t == cnt && i + 1 == cnt) s_c = double(Ci[j]) * G;
+        }
+        if (tid == 0 && t == pos) s_c = c;                           // no element on this grid
+        __syncthreads();
+        if (t >= cnt) { c = s_c; __syncthreads(); break; }
+        // step t with a real FP64 addition (the reference's own rounding)
+        if (tid == t / kEPT) {
+            double prev = s_c;
+            double pt = 0.0;
+#pragma unroll
+            for (int j = 0; j < kEPT; ++j)
+                if (j == int(t % kEPT)) pt = p[j];
+            double ct = __dadd_rn(prev, pt);
+            if (out) out[t] = ct;
+            s_c = ct;
+        }
+        __syncthreads();
+        c = s_c;
+        pos = t + 1;
+        __syncthreads();
+    }
+    return c;
+}
+
+__device__ __forceinline__ void load_block_p(const double2* __restrict__ amp, uint64_t base, uint32_t cnt,
+                                             const PermMap& pm, double (&p)[kEPT])
+{
+#pragma unroll
+    for (int j = 0; j < kEPT; ++j) {
+        uint32_t i = threadIdx.x * kEPT + j;
+        p[j] = i < cnt ? norm2(amp[phys_index(base + i, pm)]) : 0.0;
+    }
+}
+
+__global__ void __launch_bounds__(kBT) k_cdf_bsum(const double2* __restrict__ amp, uint64_t size, PermMap pm,
+                                                  double* __restrict__ bsum)
+{
+    __shared__ double sh[kBT / 32];
+    double p[kEPT];
+    uint64_t base = uint64_t(blockIdx.x) * kBS;
+    load_block_p(amp, base, kBS, pm, p);
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < kEPT; ++j) s += p[j];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kBT / 32; ++w) t += sh[w];
+        bsum[blockIdx.x] = t;
+    }
+}
+
+// single CTA: approximate exclusive prefix -> grid guess per block
+__global__ void __launch_bounds__(1024) k_cdf_guess(const double* __restrict__ bsum, uint32_t nb, int32_t* guess)
+{
+    __shared__ double part[1024];
+    const uint32_t per = (nb + blockDim.x - 1) / blockDim.x;
+    const uint32_t lo = threadIdx.x * per, hi = min(nb, lo + per);
+    double s = 0.0;
+    for (uint32_t b = lo; b < hi; ++b) s += bsum[b];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double run = 0.0;
+        for (uint32_t t = 0; t < blockDim.x; ++t) {
+            double v = part[t];
+            part[t] = run;
+            run += v;
+        }
+    }
+    __syncthreads();
+    double run = part[threadIdx.x];
+    for (uint32_t b = lo; b < hi; ++b) {
+        double lo_c = run, hi_c = run + bsum[b];
+        // conservative slack for the difference between this sum and the sequential one
+        double slack = hi_c * 0x1.0p-20 + 1e-300;
+        int e1 = lo_c - slack > 2.2250738585072014e-308 ? ilogb(lo_c - slack) : -1022;
+        int e2 = hi_c + slack > 2.2250738585072014e-308 ? ilogb(hi_c + slack) : -1022;
+        guess[b] = (e1 == e2) ? e1 : INT32_MIN;
+        run = hi_c;
+    }
+}
+
+__global__ void __launch_bounds__(kBT) k_cdf_summ(const double2* __restrict__ amp, PermMap pm,
+                                                  const int32_t* __restrict__ guess, Summ* __restrict__ summ)
+{
+    __shared__ uint64_t sh[160];
+    const int32_t e = guess[blockIdx.x];
+    if (e == INT32_MIN) {
+        if (threadIdx.x == 0) summ[blockIdx.x] = Summ{0, 0, e, 0};
+        return;
+    }
+    double p[kEPT];
+    load_block_p(amp, uint64_t(blockIdx.x) * kBS, kBS, pm, p);
+    uint64_t t0 = 0, t1 = 0;
+    int ok = 1;
+#pragma unroll
+    for (int j = 0; j < kEPT; ++j) {
+        uint64_t a0, a1, r0, r1;
+        if (!elem_map(p[j], e, a0, a1)) ok = 0;
+        compose(t0, t1, a0, a1, r0, r1);
+        t0 = r0;
+        t1 = r1;
+    }
+    ok = __syncthreads_and(ok);
+    uint64_t ex0, ex1;
+    block_scan_maps(t0, t1, ex0, ex1, sh);
+    if (threadIdx.x == blockDim.x - 1) {
+        uint64_t r0, r1;
+        compose(ex0, ex1, t0, t1, r0, r1);
+        summ[blockIdx.x] = Summ{r0, r1, e, ok};
+    }
+}
+
+// single CTA: exact running sum block by block; blocks whose guess does not
+// hold are folded exactly here.  cin[b] = exact sum before block b; cin[nb] = total.
+__global__ void __launch_bounds__(kBT) k_cdf_chain(const double2* __restrict__ amp, PermMap pm,
+                                                   const Summ* __restrict__ summ, uint32_t nb, double* __restrict__ cin)
+{
+    __shared__ uint64_t sh[160];
+    __shared__ double s_c;
+    __shared__ int s_slow;
+    if (threadIdx.x == 0) s_c = 0.0;
+    __syncthreads();
+    for (uint32_t b = 0; b < nb; ++b) {
+        if (threadIdx.x == 0) {
+            double c = s_c;
+            cin[b] = c;
+            Summ s = summ[b];
+            int slow = 1;
+            if (s.ok && s.e != INT32_MIN && c > 0.0 && epoch_of(c) == s.e) {
+                uint64_t C = uint64_t(ldexp(c, 52 - s.e));
+                uint64_t Co = C + ((C & 1) ? s.d1 : s.d0);
+                if (Co < kTwo53 && Co >= C) {
+                    s_c = ldexp(double(Co), s.e - 52);
+                    slow = 0;
+                }
+            }
+            s_slow = slow;
+        }
+        __syncthreads();
+        if (s_slow) {
+            double p[kEPT];
+            load_block_p(amp, uint64_t(b) * kBS, kBS, pm, p);
+            double c = block_exact(p, kBS, s_c, nullptr, sh);
+            if (threadIdx.x == 0) s_c = c;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) cin[nb] = s_c;
+}
+
+__global__ void __launch_bounds__(kBT) k_cdf_write(const double2* __restrict__ amp, PermMap pm,
+                                                   const double* __restrict__ cin, double* __restrict__ cdf)
+{
+    __shared__ uint64_t sh[160];
+    double p[kEPT];
+    load_block_p(amp, uint64_t(blockIdx.x) * kBS, kBS, pm, p);
+    block_exact(p, kBS, cin[blockIdx.x], cdf + uint64_t(blockIdx.x) * kBS, sh);
+}
+
+// small states (< one block): the sequential chain itself
+__global__ void k_cdf_small(const double2* __restrict__ amp, uint64_t size, PermMap pm, double* cdf, double* cin)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double c = 0.0;
+    for (uint64_t i = 0; i < size; ++i) {
+        c = __dadd_rn(c, norm2(amp[phys_index(i, pm)]));
+        cdf[i] = c;
+    }
+    cin[0] = 0.0;
+    cin[1] = c;
+}
+
+__device__ __forceinline__ uint64_t lower_bound_dev(const double* a, uint64_t n, double target)
+{
+    uint64_t lo = 0, len = n;
+    while (len > 0) {
+        uint64_t half = len >> 1, mid = lo + half;
+        if (a[mid] < target) { lo = mid + 1; len = len - half - 1; }
+        else len = half;
+    }
+    return lo;
+}
+
+// shots: target = u * total; block by binary search over block starts, then inside the block
+__global__ void k_sample(const double* __restrict__ cdf, uint64_t size, const double* __restrict__ cin, uint32_t nb,
+                         uint32_t bs, const double* __restrict__ u, uint64_t nshots, uint64_t seed,
+                         uint64_t* __restrict__ out, PermMap pm)
+{
+    const double total = cin[nb];
+    for (uint64_t s = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; s < nshots;
+         s += uint64_t(gridDim.x) * blockDim.x) {
+        double us;
+        if (u) us = u[s];
+        else {
+            double u2;
+            philox_uniform_pair(seed, s, kTagSample, us, u2);
+        }
+        double target = __dadd_rn(__dmul_rn(us, total), 0.0);
+        // last block whose first value could be >= target: search on block ends
+        // block b's last value is cin[b+1]; find first b with cin[b+1] >= target
+        uint64_t lo = 0, len = nb;
+        while (len > 0) {
+            uint64_t half = len >> 1, mid = lo + half;
+            if (cin[mid + 1] < target) { lo = mid + 1; len = len - half - 1; }
+            else len = half;
+        }
+        uint64_t idx;
+        if (lo >= nb) idx = size;  // beyond the end: lower_bound returns size
+        else {
+            uint64_t base = lo * bs;
+            uint64_t cnt = min(uint64_t(bs), size - base);
+            idx = base + lower_bound_dev(cdf + base, cnt, target);
+        }
+        out[s] = idx;
+    }
+    (void)pm;
+}
+
+PermMap make_perm(const qse_state* st)
+{
+    PermMap pm{};
+    pm.n = st->n;
+    pm.identity = st->identity_perm() ? 1 : 0;
+    for (uint32_t q = 0; q < st->n; ++q) pm.p[q] = uint8_t(st->perm[q]);
+    return pm;
+}
+
+// Builds the exact cumulative array; returns (cdf, cin, nb, bs) in ctx scratch.
+struct CdfView {
+    double* cdf;
+    double* cin;
+    uint32_t nb;
+    uint32_t bs;
+};
+
+CdfView build_cdf(qse_state* st)
+{
+    qse_ctx* ctx = st->ctx;
+    const uint64_t size = st->size();
+    PermMap pm = make_perm(st);
+    CdfView v{};
+    if (size < uint64_t(kBS)) {
+        ctx->scratch2.reserve(size * 8 + 4 * 8);
+        v.cdf = static_cast<double*>(ctx->scratch2.ptr);
+        v.cin = v.cdf + size;
+        v.nb = 1;
+        v.bs = uint32_t(size);
+        k_cdf_small<<<1, 32, 0, ctx->stream>>>(reinterpret_cast<const double2*>(st->amp), size, pm, v.cdf, v.cin);
+        QSE_CUDA(cudaGetLastError());
+        count_launch(ctx);
+        return v;
+    }
+    const uint32_t nb = uint32_t(size / kBS);
+    // scratch2: cdf [size] | cin [nb+1] | bsum [nb] | guess [nb] | summ [nb]
+    size_t off_cin = size * 8;
+    size_t off_bsum = off_cin + (size_t(nb) + 1) * 8;
+    size_t off_guess = off_bsum + size_t(nb) * 8;
+    size_t off_summ = (off_guess + size_t(nb) * 4 + 15) & ~size_t(15);
+    size_t total = off_summ + size_t(nb) * sizeof(Summ);
+    ctx->scratch2.reserve(total);
+    char* base = static_cast<char*>(ctx->scratch2.ptr);
+    v.cdf = reinterpret_cast<double*>(base);
+    v.cin = reinterpret_cast<double*>(base + off_cin);
+    double* bsum = reinterpret_cast<double*>(base + off_bsum);
+    int32_t* guess = reinterpret_cast<int32_t*>(base + off_guess);
+    Summ* summ = reinterpret_cast<Summ*>(base + off_summ);
+    v.nb = nb;
+    v.bs = kBS;
+    const double2* amp = reinterpret_cast<const double2*>(st->amp);
+    k_cdf_bsum<<<nb, kBT, 0, ctx->stream>>>(amp, size, pm, bsum);
+    k_cdf_guess<<<1, 1024, 0, ctx->stream>>>(bsum, nb, guess);
+    k_cdf_summ<<<nb, kBT, 0, ctx->stream>>>(amp, pm, guess, summ);
+    k_cdf_chain<<<1, kBT, 0, ctx->stream>>>(amp, pm, summ, nb, v.cin);
+    k_cdf_write<<<nb, kBT, 0, ctx->stream>>>(amp, pm, v.cin, v.cdf);
+    QSE_CUDA(cudaGetLastError());
+    count_launch(ctx, 5);
+    return v;
+}
+
+__global__ void k_collapse(double2* amp, uint64_t size, uint64_t phys)
+{
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < size; i += uint64_t(gridDim.x) * blockDim.x)
+        amp[i] = make_double2(i == phys ? 1.0 : 0.0, 0.0);
+}
+
+}  // namespace
+
+void sample(qse_state* st, const double* u_host, size_t nshots, uint64_t seed, uint64_t* out_host)
+{
+    qse_ctx* ctx = st->ctx;
+    if (nshots == 0) return;
+    CdfView v = build_cdf(st);
+    // scratch: u [nshots] | out [nshots]
+    size_t ubytes = u_host ? nshots * 8 : 0;
+    ctx->scratch.reserve(ubytes + nshots * 8 + 16);
+    double* d_u = u_host ? static_cast<double*>(ctx->scratch.ptr) : nullptr;
+    uint64_t* d_out = reinterpret_cast<uint64_t*>(static_cast<char*>(ctx->scratch.ptr) + ubytes);
+    if (u_host) QSE_CUDA(cudaMemcpyAsync(d_u, u_host, ubytes, cudaMemcpyHostToDevice, ctx->stream));
+    unsigned grid = unsigned(std::min<uint64_t>((nshots + 255) / 256, uint64_t(ctx->num_sms) * 8));
+    k_sample<<<grid, 256, 0, ctx->stream>>>(v.cdf, st->size(), v.cin, v.nb, v.bs, d_u, nshots, seed, d_out,
+                                            make_perm(st));
+    QSE_CUDA(cudaGetLastError());
+    count_launch(ctx);
+    QSE_CUDA(cudaMemcpyAsync(out_host, d_out, nshots * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    QSE_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+uint64_t measure(qse_state* st, double u)
+{
+    uint64_t idx = 0;
+    sample(st, &u, 1, 0, &idx);
+    // StateVector.cpp:142-149: every amplitude 0, the outcome 1 (no phase kept)
+    uint64_t L = idx < st->size() ? idx : 0;
+    uint64_t P = logical_to_physical_index(st, L);
+    qse_ctx* ctx = st->ctx;
+    uint64_t size = st->size();
+    unsigned grid = unsigned(std::min<uint64_t>((size + 255) / 256, uint64_t(ctx->num_sms) * 32));
+    k_collapse<<<grid, 256, 0, ctx->stream>>>(reinterpret_cast<double2*>(st->amp), size, P);
+    QSE_CUDA(cudaGetLastError());
+    count_launch(ctx);
+    QSE_CUDA(cudaStreamSynchronize(ctx->stream));
+    return L;
+}
+
+double total_probability(qse_state* st)
+{
+    CdfView v = build_cdf(st);
+    double t = 0.0;
+    QSE_CUDA(cudaMemcpyAsync(&t, v.cin + v.nb, 8, cudaMemcpyDeviceToHost, st->ctx->stream));
+    QSE_CUDA(cudaStreamSynchronize(st->ctx->stream));
+    return t;
+}
+
+}  // namespace qse

@@ -1,0 +1,295 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle.
+
+Amplitudes: max abs error <= 1e-12 (the reference's KAT tolerance,
+QSETests.cpp:40).  Sample / measure outcome indices and noise decisions:
+bit-exact for the same uniform draws.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle_ffi as O
+from quantumsimevo_b200 import _lib as L
+from quantumsimevo_b200 import workloads as W
+from quantumsimevo_b200.circuit import Circuit, Device, Noise, StateVector
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def dev():
+    return Device.default()
+
+
+def run_gpu(dev, n, ops, fusion=True, k=0, max_gates=0, params=None):
+    dev.set_fusion(fusion, k, max_gates)
+    st = StateVector(n, dev)
+    ops = np.ascontiguousarray(ops)
+    p = None if params is None else np.ascontiguousarray(params, dtype=np.float64)
+    stats = L.QseExecStats()
+    L.check(L.lib.qse_execute(st.handle, L.dptr(ops), len(ops), p.ctypes.data_as(L._pd) if p is not None else None,
+                              0 if p is None else p.size, None, None, 0, C.byref(stats)))
+    out = st.download()
+    dev.set_fusion(True, 12, 0)
+    return out, stats
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 7, 10, 13])
+def test_plain_kernels_every_gate_every_qubit(dev, n):
+    ops = W.random_circuit(n, 40 * n, 100 + n)
+    got, stats = run_gpu(dev, n, ops, fusion=False)
+    assert np.max(np.abs(got - O.run(n, ops))) <= TOL
+
+
+@pytest.mark.parametrize("n,k", [(4, 4), (6, 5), (9, 9), (10, 8), (12, 12), (13, 10), (14, 12), (16, 11), (18, 12)])
+def test_fused_random_circuits(dev, n, k):
+    for rep in range(3):
+        ops = W.random_circuit(n, 25 * n, 3000 + 7 * n + rep)
+        got, stats = run_gpu(dev, n, ops, fusion=True, k=k)
+        err = np.max(np.abs(got - O.run(n, ops)))
+        assert err <= TOL, (rep, err, stats.passes)
+
+
+def test_fused_gate_cap_and_tiles(dev):
+    n = 15
+    ops = W.random_circuit(n, 400, 42)
+    want = O.run(n, ops)
+    for k, cap in [(9, 3), (10, 0), (11, 17), (12, 1)]:
+        got, _ = run_gpu(dev, n, ops, k=k, max_gates=cap)
+        assert np.max(np.abs(got - want)) <= TOL
+
+
+def test_layered_rotations_16q_full(dev):
+    ops = W.layered_rotations(16, 20, seed=1)
+    got, stats = run_gpu(dev, 16, ops)
+    assert np.max(np.abs(got - O.run(16, ops))) <= TOL
+    assert stats.passes < 20
+
+
+def test_qft_20q(dev):
+    ops = W.hrz_qft(20, seed=2)
+    got, stats = run_gpu(dev, 20, ops)
+    assert np.max(np.abs(got - O.run(20, ops))) <= TOL
+    assert stats.passes <= 4
+
+
+def test_execute_twice_and_swap_relabel(dev):
+    # Circuit::execute does not clear its queue: a second execute applies it again
+    n = 11
+    ops = W.random_circuit(n, 120, 5)
+    c = Circuit(n, device=dev, seed=3)
+    c.add_ops(ops)
+    c.execute()
+    c.execute()
+    want = O.run_on(O.run(n, ops), n, ops)
+    assert np.max(np.abs(c.get_state_vector() - want)) <= TOL
+
+
+def test_per_gate_api_after_fused_relabel(dev):
+    # a fused execute leaves a qubit relabelling; per-gate calls must honour it
+    n = 10
+    ops = W.to_array([(L.SWAP, 0, 9, -1, 0, 0.0, 1.0, (0.0,) * 8), (L.H, 0, 0, -1, 0, 0.0, 1.0, (0.0,) * 8),
+                      (L.SWAP, 1, 5, -1, 0, 0.0, 1.0, (0.0,) * 8)])
+    st = StateVector(n, dev)
+    L.check(L.lib.qse_execute(st.handle, L.dptr(ops), len(ops), None, 0, None, None, 0, None))
+    L.check(L.lib.qse_apply_rx(st.handle, 0, 0.3))
+    L.check(L.lib.qse_apply_cnot(st.handle, 0, 5))
+    more = W.to_array([(L.RX, 0, 0, -1, 0, 0.3, 1.0, (0.0,) * 8), (L.CNOT, 5, 0, -1, 0, 0.0, 1.0, (0.0,) * 8)])
+    want = O.run(n, np.concatenate([ops, more]))
+    assert np.max(np.abs(st.download() - want)) <= TOL
+    L.check(L.lib.qse_state_canonicalize(st.handle))
+    assert st.qubit_map() == list(range(n))
+    assert np.max(np.abs(st.download() - want)) <= TOL
+
+
+def test_errors_are_status_codes(dev):
+    st = StateVector(4, dev)
+    assert L.lib.qse_apply_h(st.handle, 4) == 2
+    ops = L.as_ops([L.make_op(L.CNOT, 1, 9)])
+    assert L.lib.qse_execute(st.handle, L.dptr(ops), 1, None, 0, None, None, 0, None) == 2
+    h = C.c_void_p()
+    assert L.lib.qse_state_create(dev.handle, 80, C.byref(h)) == 5
+    # the context is still usable
+    L.check(L.lib.qse_apply_h(st.handle, 3))
+
+
+# ---------------------------------------------------------------- sampling
+def boundary_uniforms(st, n, count, seed):
+    """Uniforms that put targets exactly on and next to cumulative values."""
+    cum = O.cdf(st, n)
+    total = cum[-1]
+    rng = np.random.default_rng(seed)
+    picks = rng.integers(0, cum.size, count)
+    u = []
+    for i in picks:
+        x = cum[i] / total
+        for v in (x, np.nextafter(x, 0.0), np.nextafter(x, 1.0)):
+            if 0.0 <= v < 1.0:
+                u.append(v)
+    u += list(rng.random(count))
+    return np.array(u, dtype=np.float64)
+
+
+@pytest.mark.parametrize("n", [1, 3, 8, 11, 12, 13, 16, 20])
+def test_sample_bit_exact(dev, n):
+    ops = W.random_circuit(n, 20 * n, 600 + n)
+    c = Circuit(n, device=dev, seed=9)
+    c.add_ops(ops)
+    c.execute()
+    st = O.run(n, ops)
+    u = boundary_uniforms(st, n, 300, n)
+    got = c.sample(len(u), uniforms=u)
+    want = O.sample(st, n, u)
+    assert np.array_equal(got, want)
+
+
+def test_sample_exact_cdf_many_binades(dev):
+    # amplitudes spread over many binades so the running sum crosses many
+    # binade boundaries inside blocks (the exact scan's slow path)
+    n = 16
+    rng = np.random.default_rng(5)
+    mag = np.exp(rng.uniform(-60, 0, 1 << n))
+    amp = mag * np.exp(1j * rng.uniform(0, 2 * np.pi, 1 << n))
+    amp[:100] = 0.0
+    amp[5000:5003] = 1e-160
+    st = StateVector(n, dev)
+    st.upload(amp)
+    u = boundary_uniforms(amp, n, 500, 1)
+    out = np.empty(len(u), dtype=np.uint64)
+    L.check(L.lib.qse_sample(st.handle, u.ctypes.data_as(L._pd), len(u), 0, out.ctypes.data_as(L._pu64)))
+    assert np.array_equal(out, O.sample(amp, n, u))
+    t = C.c_double()
+    L.check(L.lib.qse_total_probability(st.handle, C.byref(t)))
+    assert t.value == O.cdf(amp, n)[-1]
+
+
+def test_sample_ties_to_even(dev):
+    # probabilities that are exact multiples of half-ulps exercise the tie rule
+    n = 14
+    p = np.full(1 << n, 2.0 ** -14)
+    p[1::3] = 2.0 ** -14 + 2.0 ** -67
+    amp = np.sqrt(p).astype(np.complex128)
+    st = StateVector(n, dev)
+    st.upload(amp)
+    u = boundary_uniforms(amp, n, 400, 2)
+    out = np.empty(len(u), dtype=np.uint64)
+    L.check(L.lib.qse_sample(st.handle, u.ctypes.data_as(L._pd), len(u), 0, out.ctypes.data_as(L._pu64)))
+    assert np.array_equal(out, O.sample(amp, n, u))
+
+
+def test_measure_collapses(dev):
+    n = 12
+    ops = W.random_circuit(n, 200, 8)
+    c = Circuit(n, device=dev, seed=1)
+    c.add_ops(ops)
+    c.execute()
+    st = O.run(n, ops)
+    u = 0.6180339887
+    idx_want, st_want = O.measure(st, n, u)
+    assert c.measure(u) == idx_want
+    assert np.array_equal(c.get_state_vector(), st_want)
+
+
+def test_sample_after_relabel_is_logical(dev):
+    n = 13
+    ops = np.concatenate([W.random_circuit(n, 100, 12), W.to_array(W.qft_ops(n))])
+    c = Circuit(n, device=dev, seed=2)
+    c.add_ops(ops)
+    c.execute()
+    st = O.run(n, ops)
+    u = boundary_uniforms(st, n, 200, 3)
+    assert np.array_equal(c.sample(len(u), uniforms=u), O.sample(st, n, u))
+
+
+# ---------------------------------------------------------------- noise
+def _noisy(dev, n, ops, rng_mode, seed=42, mult=1.0, uniforms=None, rates=None):
+    nz = Noise(n, seed, mult, rng_mode, rates=rates, device=dev)
+    st = StateVector(n, dev)
+    u = None if uniforms is None else np.ascontiguousarray(uniforms, dtype=np.float64)
+    stats = L.QseExecStats()
+    L.check(L.lib.qse_execute(st.handle, L.dptr(ops), len(ops), None, 0, nz.handle,
+                              u.ctypes.data_as(L._pd) if u is not None else None, 0 if u is None else u.size,
+                              C.byref(stats)))
+    return st.download(), nz.counts(), stats
+
+
+@pytest.mark.parametrize("n", [5, 12])
+def test_noise_injected_uniforms_bit_exact(dev, n):
+    ops = W.random_circuit(n, 300, 70 + n)
+    rates = W.noise_rates(1e-3)
+    cfg = L.default_noise_config(True, L.RNG_INJECTED, 42, 50.0, rates)
+    noisy = int(np.sum(np.isin(ops["type"], list(rates))))
+    u = np.random.default_rng(n).random(2 * noisy)
+    st_want, nz = O.execute_noisy(n, ops, cfg, uniforms=u)
+    st, (bits, phases), stats = _noisy(dev, n, ops, L.RNG_INJECTED, mult=50.0, uniforms=u, rates=rates)
+    assert stats.noisy_gates == noisy
+    assert bits == list(nz.bit[:n]) and phases == list(nz.phase[:n])
+    assert sum(bits) > 0
+    assert np.max(np.abs(st - st_want)) <= TOL
+
+
+def test_noise_philox_matches_oracle_philox(dev):
+    n = 10
+    ops = W.random_circuit(n, 500, 71)
+    cfg = L.default_noise_config(True, L.RNG_PHILOX, 1234, 100.0)
+    st_want, nz = O.execute_noisy(n, ops, cfg)
+    st, (bits, phases), _ = _noisy(dev, n, ops, L.RNG_PHILOX, seed=1234, mult=100.0)
+    assert bits == list(nz.bit[:n]) and phases == list(nz.phase[:n])
+    assert np.max(np.abs(st - st_want)) <= TOL
+
+
+def test_noise_mt19937_matches_reference_stream(dev):
+    # QSE_RNG_MT19937 consumes mt19937(42) like Noise.cpp; counts match the oracle's restatement
+    n = 8
+    ops = W.random_circuit(n, 400, 72)
+    cfg = L.default_noise_config(True, L.RNG_MT19937, 42, 30.0)
+    st_want, nz = O.execute_noisy(n, ops, cfg)
+    st, (bits, phases), _ = _noisy(dev, n, ops, L.RNG_MT19937, seed=42, mult=30.0)
+    assert bits == list(nz.bit[:n]) and phases == list(nz.phase[:n])
+    assert np.max(np.abs(st - st_want)) <= TOL
+
+
+# ---------------------------------------------------------------- gradients
+def _adjoint(dev, n, ops, params, obs_t):
+    obs, keep = L.observable(*obs_t)
+    st = StateVector(n, dev)
+    p = np.ascontiguousarray(params, dtype=np.float64)
+    g = np.zeros(p.size)
+    v = C.c_double()
+    L.check(L.lib.qse_adjoint(st.handle, L.dptr(ops), len(ops), p.ctypes.data_as(L._pd), p.size, C.byref(obs),
+                              C.byref(v), g.ctypes.data_as(L._pd)))
+    return v.value, g
+
+
+@pytest.mark.parametrize("n", [6, 10, 12])
+def test_adjoint_qaoa_vs_oracle(dev, n):
+    ops, params, edges, obs_t = W.qaoa_maxcut(n, 3, seed=40 + n)
+    v, g = _adjoint(dev, n, ops, params, obs_t)
+    obs, keep = L.observable(*obs_t)
+    vw, gw = O.adjoint(n, ops, params, obs)
+    vs, gs = O.param_shift(n, ops, params, obs)
+    assert abs(v - vw) <= 1e-10
+    assert np.max(np.abs(g - gw)) <= 1e-10
+    assert np.max(np.abs(g - gs)) <= 1e-10
+
+
+def test_adjoint_every_parameterised_type(dev):
+    n = 9
+    rng = W.SplitMix64(33)
+    base = W.random_circuit(n, 80, 34, with_2x2=True)
+    ops = base.copy()
+    nparam = 0
+    for i in range(len(ops)):
+        if int(ops[i]["type"]) in (L.RX, L.RY, L.RZ, L.PHASE, L.CPHASE, L.MCPHASE):
+            ops[i]["param"] = nparam % 7
+            ops[i]["coeff"] = 0.5 + rng.uniform()
+            nparam += 1
+    params = np.array([rng.uniform() * 6.28 for _ in range(7)])
+    obs_t = ([1 << q for q in range(n)] + [3, 0b101000], [1.0] * n + [0.25, -0.7], 0.3)
+    v, g = _adjoint(dev, n, ops, params, obs_t)
+    obs, keep = L.observable(*obs_t)
+    vw, gw = O.adjoint(n, ops, params, obs)
+    assert abs(v - vw) <= 1e-10
+    assert np.max(np.abs(g - gw)) <= 1e-10

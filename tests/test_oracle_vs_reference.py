@@ -1,0 +1,97 @@
+"""The oracle restatement against the reference engine itself (CPU only):
+committed golden outputs of the reference (tests/golden/make_golden.py) and,
+when the reference was compiled in this checkout (oracle/_ref), live runs."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import oracle_ffi as O
+from quantumsimevo_b200 import _lib as L
+from quantumsimevo_b200 import workloads as W
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _circuits():
+    d = np.load(os.path.join(GOLD, "ref_circuits.npz"))
+    return [(int(d[f"c{i}_n"]), d[f"c{i}_ops"], d[f"c{i}_state"]) for i in range(int(d["count"]))]
+
+
+@pytest.mark.parametrize("idx", range(21))
+def test_oracle_matches_reference_golden(idx):
+    n, ops, want = _circuits()[idx]
+    got = O.run(n, ops)
+    # same arithmetic order, compiled without FMA contraction: bit for bit
+    assert np.array_equal(got, want), np.max(np.abs(got - want))
+
+
+def test_noise_oracle_matches_reference_golden():
+    d = np.load(os.path.join(GOLD, "ref_noise.npz"))
+    for k in range(int(d["count"])):
+        n = int(d[f"k{k}_n"])
+        cfg = L.default_noise_config(True, L.RNG_MT19937, 42, float(d[f"k{k}_mult"]))
+        nz = O.OrcNoise()
+        O.oracle.orc_noise_init(C.byref(nz), n, C.byref(cfg))
+        for t, q in zip(d[f"k{k}_types"], d[f"k{k}_targets"]):
+            # accumulate only (identity gates keep the state): drive orc_execute with one IDENTITY op per draw
+            op = W.to_array([(int(t), int(q), 0, -1, 0, 0.0, 1.0, (0.0,) * 8)])
+            op["type"][0] = int(t)
+            # consume the draws exactly like Noise::accumulateError
+            O.oracle.orc_noise_accumulate = getattr(O.oracle, "orc_noise_accumulate")
+            O.oracle.orc_noise_accumulate.argtypes = [C.POINTER(O.OrcNoise), C.c_int, C.c_uint, C.c_void_p]
+            O.oracle.orc_noise_accumulate(C.byref(nz), int(t), int(q), None)
+        st = np.ascontiguousarray(d[f"k{k}_in"]).copy()
+        O.oracle.orc_noise_apply.argtypes = [C.POINTER(O.OrcNoise), C.c_void_p]
+        O.oracle.orc_noise_apply(C.byref(nz), st.ctypes.data_as(C.c_void_p))
+        assert sum(nz.bit[:n]) == int(d[f"k{k}_bits"])
+        assert sum(nz.phase[:n]) == int(d[f"k{k}_phases"])
+        assert np.array_equal(st, d[f"k{k}_out"])
+
+
+@pytest.fixture(scope="module")
+def ref():
+    r = O.load_reference(gpu=False)
+    if r is None:
+        pytest.skip("reference not compiled in this checkout (make -C oracle ref)")
+    r.ref_set_quiet(1)
+    return r
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 7, 9, 11])
+def test_oracle_matches_live_reference_scalar(ref, n):
+    for rep in range(3):
+        ops = W.random_circuit(n, 30 + 10 * n, 500 + 31 * n + rep, with_2x2=False)
+        assert np.array_equal(O.run(n, ops), O.ref_run(ref, n, ops, backend=0))
+
+
+@pytest.mark.parametrize("n", [2, 4, 6, 8])
+def test_reference_avx_backend_close_except_z_q0(ref, n):
+    # The AVX2 backend (the timed CPU baseline) agrees with the scalar one to
+    # rounding, except applyPauliZ on qubit 0, which its loop never reaches
+    # (CircuitUnitaryOperationAVX.cpp:131-138).
+    ops = W.random_circuit(n, 40, 900 + n, with_2x2=False)
+    ops = ops[~((ops["type"] == L.Z) & (ops["target"] == 0))]
+    a = O.ref_run(ref, n, ops, backend=0)
+    b = O.ref_run(ref, n, ops, backend=1)
+    assert np.max(np.abs(a - b)) < 1e-13
+    z0 = W.to_array([(L.H, 0, 0, -1, 0, 0.0, 1.0, (0.0,) * 8), (L.Z, 0, 0, -1, 0, 0.0, 1.0, (0.0,) * 8)])
+    assert not np.allclose(O.ref_run(ref, n, z0, backend=0), O.ref_run(ref, n, z0, backend=1))
+
+
+def test_reference_sample_matches_lower_bound_semantics(ref):
+    # StateVector::sample draws are from random_device, so only the support can be checked
+    n = 6
+    ops = W.random_circuit(n, 40, 77, with_2x2=False)
+    st = O.run(n, ops)
+    assert ref.ref_set_backend(0) == 0
+    h = ref.ref_circuit_new(n, 0)
+    a = np.ascontiguousarray(ops)
+    ref.ref_circuit_add_many(h, a.ctypes.data_as(C.c_void_p), len(a))
+    ref.ref_circuit_execute(h, 0)
+    out = np.empty(2000, dtype=np.uint64)
+    ref.ref_circuit_sample(h, 2000, out.ctypes.data_as(C.POINTER(C.c_uint64)))
+    ref.ref_circuit_free(h)
+    p = np.abs(st) ** 2
+    assert np.all(p[out.astype(np.int64)] > 0)
