@@ -188,7 +188,7 @@ int qse_ctx_set_fusion(qse_ctx* ctx, int enabled, int tile_qubits, int max_gates
 {
     QSE_GUARD_BEGIN
     need(ctx != nullptr, QSE_ERR_INVALID, "null context");
-    need(tile_qubits == 0 || (tile_qubits >= 5 && tile_qubits <= 12), QSE_ERR_INVALID, "tile_qubits must be 5..12");
+    need(tile_qubits == 0 || (tile_qubits >= 4 && tile_qubits <= 12), QSE_ERR_INVALID, "tile_qubits must be 4..12");
     need(max_gates_per_pass >= 0, QSE_ERR_INVALID, "max_gates_per_pass must be >= 0");
     ctx->fusion = enabled ? 1 : 0;
     if (tile_qubits) ctx->tile_qubits = tile_qubits;

@@ -115,7 +115,7 @@ public:
         need_ = &need;
         choose_regs(0, nullptr);
         P.layout0 = add_layout(nullptr);
-        double scale = 1.0;
+        scale_ = 1.0;
         for (size_t i = 0; i < abs.size(); ++i) {
             const Absorbed& a = abs[i];
             const Gate& g = *a.g;
@@ -146,7 +146,7 @@ public:
                 set_control(op, a.pc);
             } else {
                 switch (g.type) {
-                case QSE_GATE_H: op.kind = K_H; scale *= kInvSqrt2; break;
+                case QSE_GATE_H: op.kind = K_H; scale_ *= kInvSqrt2; break;
                 case QSE_GATE_X: op.kind = K_X; break;
                 case QSE_GATE_Y: op.kind = K_Y; break;
                 case QSE_GATE_RX: op.kind = K_RX; op.a = std::cos(g.theta / 2.0); op.b = std::sin(g.theta / 2.0); break;
@@ -162,7 +162,7 @@ public:
             P.ops.push_back(op);
             P.n_nondiag++;
         }
-        close_all(true, scale * std::cos(gphase_), scale * std::sin(gphase_));
+        close_all(true, scale_ * std::cos(gphase_), scale_ * std::sin(gphase_));
     }
 
 private:
@@ -175,6 +175,7 @@ private:
     int nthr_ = 0;
     const std::vector<int>* need_ = nullptr;
     double gphase_ = 0.0;
+    double scale_ = 1.0;   // product of the 1/sqrt2 factors of the unscaled K_H applied so far
 
     struct OG {
         uint8_t kind, p, f;
@@ -404,6 +405,7 @@ private:
         else if (g.type == QSE_GATE_RY) op.kind = K_GRAD_Y;
         else return;
         op.g = new_slot(g.grad);
+        op.a = scale_ * scale_;   // both states still lack the pass's pending H scale
         P.ops.push_back(op);
     }
 
@@ -423,6 +425,7 @@ private:
             return;
         }
         op.g = new_slot(g.grad);
+        op.a = scale_ * scale_;   // both states still lack the pass's pending H scale
         P.ops.push_back(op);
     }
 };

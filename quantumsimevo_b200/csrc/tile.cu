@@ -294,7 +294,7 @@ __global__ void __launch_bounds__(256, 2) k_tile(const PassArgs A)
     const uint32_t warp = tid >> 5, lane = tid & 31;
 
     __shared__ uint8_t s_tile[16];
-    if (tid < 16) s_tile[tid] = A.tile_phys[tid];
+    for (uint32_t i = tid; i < 16; i += blockDim.x) s_tile[i] = A.tile_phys[i];
 
     // outer bits of this CTA
     uint64_t obase = 0;
@@ -481,7 +481,7 @@ __global__ void __launch_bounds__(256, 2) k_tile(const PassArgs A)
                             if ((j & op.f) == op.f) part += im_ls(a[1][j], a[0][j]);
                     }
                 }
-                part = warp_sum(part);
+                part = warp_sum(part * op.a);
                 if (lane == 0) wpart[op.g * nwarps + warp] += part;
             }
             break;
@@ -513,8 +513,10 @@ void launch_t(qse_ctx* ctx, const PassArgs& a, uint32_t n, size_t smem)
     static bool configured[64] = {false};
     int dev = ctx->device;
     if (!configured[dev & 63]) {
+        cudaFuncAttributes fa{};
+        QSE_CUDA(cudaFuncGetAttributes(&fa, k_tile<RB, NS>));
         QSE_CUDA(cudaFuncSetAttribute(k_tile<RB, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      int(ctx->smem_optin)));
+                                      int(ctx->smem_optin - fa.sharedSizeBytes)));
         configured[dev & 63] = true;
     }
     uint32_t threads = 1u << (a.k - RB);
