@@ -140,6 +140,16 @@ QSE_API int qse_ctx_set_fusion(qse_ctx* ctx, int enabled, int tile_qubits, int m
 QSE_API int qse_ctx_set_sample_mode(qse_ctx* ctx, int mode);
 /* number of kernels this context has launched so far */
 QSE_API uint64_t qse_ctx_kernel_launches(const qse_ctx* ctx);
+/* Timing on the context's stream (print_steps / benchmarks, like
+ * CircuitUnitaryOperationGPU::timedLaunchStart/End, CircuitUnitaryOperationGPU.cu:194-207):
+ * record event `slot` (0..63); elapsed milliseconds between two recorded slots. */
+QSE_API int qse_ctx_record(qse_ctx* ctx, int slot);
+QSE_API int qse_ctx_elapsed(qse_ctx* ctx, int slot_a, int slot_b, float* ms);
+/* Per-launch device time of the fused pass kernel: when enabled, every pass
+ * launch is bracketed by events on the launching stream; qse_ctx_pass_times
+ * returns (and clears) the count and summed milliseconds. */
+QSE_API int qse_ctx_time_passes(qse_ctx* ctx, int enabled);
+QSE_API int qse_ctx_pass_times(qse_ctx* ctx, uint64_t* launches, double* total_ms);
 
 /* ---- state vector ---------------------------------------------------- */
 /* StateVector::StateVector (StateVector.cpp:14-32): 2^n amplitudes, |0..0>. Device-resident. */
@@ -204,6 +214,16 @@ QSE_API int qse_plan_describe(uint32_t nqubits, const qse_op* ops, size_t nops, 
                               size_t nparams, uint32_t tile_qubits, uint32_t max_gates_per_pass,
                               char* buf, size_t buflen, size_t* needed);
 
+/* Pass kernels: 1 (default) = each planned pass is specialised into its own
+ * kernel and compiled for sm_100a at run time (cached by source); 0 = one
+ * generic kernel interprets the pass program. */
+QSE_API int qse_ctx_set_jit(qse_ctx* ctx, int enabled);
+/* Generates and compiles (no GPU needed, nothing loaded) every pass kernel the
+ * planner makes for ops: nstates 1 = forward passes, 2 = adjoint reverse
+ * passes.  *source_bytes receives the total generated source size. */
+QSE_API int qse_plan_compile(uint32_t nqubits, const qse_op* ops, size_t nops, const double* params,
+                             size_t nparams, uint32_t tile_qubits, int nstates, size_t* source_bytes);
+
 /* ---- StateVector::sample / measure (StateVector.cpp:77-156), on the device ----
  * Outcome = first index i whose inclusive cumulative probability (summed in
  * index order with FP64 rounding after every addition, exactly as the
@@ -212,6 +232,10 @@ QSE_API int qse_plan_describe(uint32_t nqubits, const qse_op* ops, size_t nops, 
  * Results are logical basis indices. */
 QSE_API int qse_sample(qse_state* st, const double* uniforms, size_t nshots, uint64_t seed,
                        uint64_t* out_indices);
+/* Device-resident variant: d_uniforms (or NULL for Philox(seed)) and d_out are
+ * device pointers; enqueued on the context stream, no host synchronisation. */
+QSE_API int qse_sample_device(qse_state* st, const double* d_uniforms, size_t nshots, uint64_t seed,
+                              uint64_t* d_out);
 /* measure(): outcome for uniform u, then collapse to |outcome> (amplitude 1, all others 0) */
 QSE_API int qse_measure(qse_state* st, double u, uint64_t* out_index);
 /* total probability as the reference's sequential loop rounds it */

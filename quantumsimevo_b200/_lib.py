@@ -84,6 +84,11 @@ _SIGS = {
     "qse_ctx_set_fusion": ([_vp, C.c_int, C.c_int, C.c_int], C.c_int),
     "qse_ctx_set_sample_mode": ([_vp, C.c_int], C.c_int),
     "qse_ctx_kernel_launches": ([_vp], _u64),
+    "qse_ctx_record": ([_vp, C.c_int], C.c_int),
+    "qse_ctx_elapsed": ([_vp, C.c_int, C.c_int, C.POINTER(C.c_float)], C.c_int),
+    "qse_ctx_time_passes": ([_vp, C.c_int], C.c_int),
+    "qse_ctx_pass_times": ([_vp, _pu64, _pd], C.c_int),
+    "qse_sample_device": ([_vp, _vp, _sz, _u64, _vp], C.c_int),
     "qse_state_create": ([_vp, _u32, C.POINTER(_vp)], C.c_int),
     "qse_state_destroy": ([_vp], C.c_int),
     "qse_state_qubits": ([_vp], _u32),
@@ -189,3 +194,11 @@ def default_noise_config(enabled=True, rng_mode=RNG_PHILOX, seed=42, multiplier=
     for i in range(16):
         cfg.rates[i] = r[i]
     return cfg
+
+for _name, (_args, _res) in {
+    "qse_ctx_set_jit": ([_vp, C.c_int], C.c_int),
+    "qse_plan_compile": ([_u32, _vp, _sz, _pd, _sz, _u32, C.c_int, C.POINTER(_sz)], C.c_int),
+}.items():
+    _f = getattr(lib, _name)
+    _f.argtypes = _args
+    _f.restype = _res

@@ -9,6 +9,7 @@
 #include <new>
 #include <string>
 
+#include "jit.h"
 #include "planner.h"
 #include "qse_internal.h"
 
@@ -170,6 +171,9 @@ int qse_ctx_destroy(qse_ctx* ctx)
     ctx->host_small.release();
     ctx->host_small2.release();
     if (ctx->plan_event) cudaEventDestroy(ctx->plan_event);
+    for (cudaEvent_t e : ctx->slots)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->pass_events) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     QSE_GUARD_END
@@ -206,6 +210,53 @@ int qse_ctx_set_sample_mode(qse_ctx* ctx, int mode)
 }
 
 uint64_t qse_ctx_kernel_launches(const qse_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+int qse_ctx_record(qse_ctx* ctx, int slot)
+{
+    QSE_GUARD_BEGIN
+    need(ctx != nullptr && slot >= 0 && slot < 64, QSE_ERR_INVALID, "bad context or slot");
+    bind_device(ctx);
+    if (!ctx->slots[slot]) QSE_CUDA(cudaEventCreate(&ctx->slots[slot]));
+    QSE_CUDA(cudaEventRecord(ctx->slots[slot], ctx->stream));
+    QSE_GUARD_END
+}
+
+int qse_ctx_elapsed(qse_ctx* ctx, int a, int b, float* ms)
+{
+    QSE_GUARD_BEGIN
+    need(ctx && ms && a >= 0 && a < 64 && b >= 0 && b < 64, QSE_ERR_INVALID, "bad argument");
+    need(ctx->slots[a] && ctx->slots[b], QSE_ERR_STATE, "slot never recorded");
+    bind_device(ctx);
+    QSE_CUDA(cudaEventSynchronize(ctx->slots[b]));
+    QSE_CUDA(cudaEventElapsedTime(ms, ctx->slots[a], ctx->slots[b]));
+    QSE_GUARD_END
+}
+
+int qse_ctx_time_passes(qse_ctx* ctx, int enabled)
+{
+    QSE_GUARD_BEGIN
+    need(ctx != nullptr, QSE_ERR_INVALID, "null context");
+    ctx->time_passes = enabled != 0;
+    QSE_GUARD_END
+}
+
+int qse_ctx_pass_times(qse_ctx* ctx, uint64_t* launches, double* total_ms)
+{
+    QSE_GUARD_BEGIN
+    need(ctx && launches && total_ms, QSE_ERR_INVALID, "null argument");
+    bind_device(ctx);
+    QSE_CUDA(cudaStreamSynchronize(ctx->stream));
+    double t = 0.0;
+    for (size_t i = 0; i + 1 < ctx->pass_events_used; i += 2) {
+        float ms = 0.f;
+        QSE_CUDA(cudaEventElapsedTime(&ms, ctx->pass_events[i], ctx->pass_events[i + 1]));
+        t += ms;
+    }
+    *launches = ctx->pass_events_used / 2;
+    *total_ms = t;
+    ctx->pass_events_used = 0;
+    QSE_GUARD_END
+}
 
 int qse_state_create(qse_ctx* ctx, uint32_t nqubits, qse_state** out)
 {
@@ -265,6 +316,7 @@ int qse_state_upload(qse_state* st, const double* host)
     need(st != nullptr && host != nullptr, QSE_ERR_INVALID, "null argument");
     bind_device(st->ctx);
     for (uint32_t q = 0; q < 64; ++q) st->perm[q] = q;
+    st->touch();
     QSE_CUDA(cudaMemcpyAsync(st->amp, host, st->size() * 16, cudaMemcpyHostToDevice, st->ctx->stream));
     QSE_CUDA(cudaStreamSynchronize(st->ctx->stream));
     QSE_GUARD_END
@@ -449,6 +501,55 @@ int qse_plan_describe(uint32_t nqubits, const qse_op* ops, size_t nops, const do
     QSE_GUARD_END
 }
 
+int qse_ctx_set_jit(qse_ctx* ctx, int enabled)
+{
+    QSE_GUARD_BEGIN
+    need(ctx != nullptr, QSE_ERR_INVALID, "null context");
+    ctx->jit = enabled ? 1 : 0;
+    QSE_GUARD_END
+}
+
+int qse_plan_compile(uint32_t nqubits, const qse_op* ops, size_t nops, const double* params, size_t nparams,
+                     uint32_t tile_qubits, int nstates, size_t* source_bytes)
+{
+    QSE_GUARD_BEGIN
+    need(nqubits >= 3 && nqubits <= 40, QSE_ERR_SIZE, "qubit count out of range");
+    need(nops == 0 || ops != nullptr, QSE_ERR_INVALID, "null ops");
+    need(nstates == 1 || nstates == 2, QSE_ERR_INVALID, "nstates must be 1 or 2");
+    std::vector<qse::plan::Gate> gates;
+    for (size_t i = 0; i < nops; ++i) {
+        size_t k = nstates == 2 ? nops - 1 - i : i;
+        qse::plan::Gate g;
+        g.type = ops[k].type;
+        g.t = ops[k].target;
+        g.c = ops[k].control;
+        g.cmask = ops[k].controls;
+        g.theta = qse::bound_angle(ops[k], params, nparams);
+        std::memcpy(g.m, ops[k].m, sizeof(g.m));
+        if (nstates == 2 && ops[k].param >= 0) g.grad = int32_t(k);
+        gates.push_back(g);
+    }
+    uint32_t perm[64];
+    for (uint32_t q = 0; q < 64; ++q) perm[q] = q;
+    qse::plan::Options opt;
+    opt.rb = nstates == 2 ? 3 : 4;
+    opt.k = std::min<uint32_t>(tile_qubits ? tile_qubits : (nstates == 2 ? 11 : 12), nqubits);
+    opt.grads = nstates == 2;
+    if (nstates == 2) {
+        opt.max_terms = 512;
+        opt.max_gates = 256;
+    }
+    qse::plan::Plan pl = qse::plan::build(gates, nqubits, perm, opt);
+    size_t total = 0;
+    for (const auto& p : pl.passes) {
+        qse::jit::Source s = qse::jit::generate(p, nstates);
+        total += s.code.size();
+        qse::jit::compile_only(s);
+    }
+    if (source_bytes) *source_bytes = total;
+    QSE_GUARD_END
+}
+
 int qse_sample(qse_state* st, const double* uniforms, size_t nshots, uint64_t seed, uint64_t* out_indices)
 {
     QSE_GUARD_BEGIN
@@ -459,6 +560,16 @@ int qse_sample(qse_state* st, const double* uniforms, size_t nshots, uint64_t se
             need(uniforms[i] >= 0.0 && uniforms[i] < 1.0, QSE_ERR_INVALID, "uniforms must lie in [0,1)");
     bind_device(st->ctx);
     qse::sample(st, uniforms, nshots, seed, out_indices);
+    QSE_GUARD_END
+}
+
+int qse_sample_device(qse_state* st, const double* d_uniforms, size_t nshots, uint64_t seed, uint64_t* d_out)
+{
+    QSE_GUARD_BEGIN
+    need(st != nullptr, QSE_ERR_INVALID, "null state");
+    need(nshots == 0 || d_out != nullptr, QSE_ERR_INVALID, "null output");
+    bind_device(st->ctx);
+    qse::sample_device(st, d_uniforms, nshots, seed, d_out);
     QSE_GUARD_END
 }
 

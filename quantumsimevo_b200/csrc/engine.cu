@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 
+#include "jit.h"
 #include "planner.h"
 #include "qse_internal.h"
 #include "tile.cuh"
@@ -161,6 +162,47 @@ Uploaded upload_plan(qse_ctx* ctx, const plan::Plan& pl)
     return up;
 }
 
+// Runs the passes of a plan: specialised NVRTC kernels (jit.cpp) when the
+// context allows it, else the generic tile-program interpreter (tile.cu).
+struct PassRunner {
+    qse_ctx* ctx;
+    qse_state* st;
+    Uploaded& up;
+    int ns;
+    uint32_t rb;
+    std::vector<jit::Source> srcs;
+    std::vector<std::shared_ptr<jit::Kernel>> ks;
+    std::vector<uint32_t> kq;
+
+    PassRunner(qse_state* s, const plan::Plan& pl, Uploaded& u, int nstates, uint32_t regbits)
+        : ctx(s->ctx), st(s), up(u), ns(nstates), rb(regbits)
+    {
+        for (const auto& p : pl.passes) kq.push_back(p.k);
+        if (!ctx->jit) return;
+        srcs.reserve(pl.passes.size());
+        for (const auto& p : pl.passes) srcs.push_back(jit::generate(p, ns));
+        std::vector<const jit::Source*> ptrs;
+        for (const auto& s2 : srcs) ptrs.push_back(&s2);
+        ks = jit::get_kernels(ptrs);
+    }
+
+    void run(size_t i, double2* lam, double* part)
+    {
+        tile::PassArgs a = up.args[i];
+        a.psi = reinterpret_cast<double2*>(st->amp);
+        a.lam = lam;
+        a.slot_partial = part;
+        if (!ctx->jit) {
+            tile::launch_pass(ctx, a, st->n, rb, ns);
+            return;
+        }
+        cudaEvent_t stop = tile::pass_timer_begin(ctx);
+        jit::launch(ctx, *ks[i], srcs[i], st->n, kq[i], a.psi, lam, a.terms, a.groups, part);
+        tile::pass_timer_end(ctx, stop);
+        count_launch(ctx);
+    }
+};
+
 uint32_t tile_qubits_for(const qse_ctx* ctx, uint32_t n, uint32_t rb, uint32_t kmax)
 {
     uint32_t k = std::min<uint32_t>(std::max(ctx->tile_qubits, int(rb) + 1), kmax);
@@ -215,6 +257,7 @@ void execute_program(qse_state* st, const qse_op* ops, size_t nops, const double
     qse_ctx* ctx = st->ctx;
     const uint64_t launches0 = ctx->launches;
     if (stats) *stats = qse_exec_stats{};
+    st->touch();
     std::vector<plan::Gate> gates;
     gates.reserve(nops);
     for (size_t i = 0; i < nops; ++i) {
@@ -236,10 +279,8 @@ void execute_program(qse_state* st, const qse_op* ops, size_t nops, const double
         opt.max_gates = uint32_t(std::max(0, ctx->max_gates_per_pass));
         plan::Plan pl = plan::build(gates, st->n, st->perm, opt);
         Uploaded up = upload_plan(ctx, pl);
-        for (tile::PassArgs& a : up.args) {
-            a.psi = reinterpret_cast<double2*>(st->amp);
-            tile::launch_pass(ctx, a, st->n, 4, 1);
-        }
+        PassRunner runner(st, pl, up, 1, 4);
+        for (size_t i = 0; i < up.args.size(); ++i) runner.run(i, nullptr, nullptr);
         for (uint32_t q = 0; q < st->n; ++q) st->perm[q] = pl.perm_final[q];
         passes = pl.passes.size();
     }
@@ -255,11 +296,13 @@ void apply_single(qse_state* st, const qse_op& op)
 {
     plan::Gate g = to_gate(op, op.theta);
     check_qubits(g, st->n);
+    st->touch();
     apply_plain(st, g);
 }
 
 void canonicalize(qse_state* st)
 {
+    st->touch();
     // restore logical == physical with physical qubit swaps (each a half sweep)
     for (uint32_t q = 0; q < st->n; ++q) {
         if (st->perm[q] == q) continue;
@@ -466,12 +509,10 @@ double adjoint(qse_state* st, const qse_op* ops, size_t nops, const double* para
             std::memcpy(h + i * b_src, pl.passes[i].slot_src.data(), pl.passes[i].slot_src.size() * 4);
         QSE_CUDA(cudaMemcpyAsync(srcbase, h, b_src * pl.passes.size(), cudaMemcpyHostToDevice, ctx->stream));
     }
+    PassRunner runner(st, pl, up, 2, 3);
     for (size_t i = 0; i < up.args.size(); ++i) {
-        tile::PassArgs a = up.args[i];
-        a.psi = reinterpret_cast<double2*>(st->amp);
-        a.lam = reinterpret_cast<double2*>(st->aux);
-        a.slot_partial = part;
-        tile::launch_pass(ctx, a, st->n, 3, 2);
+        const tile::PassArgs& a = up.args[i];
+        runner.run(i, reinterpret_cast<double2*>(st->aux), part);
         if (a.nslots) {
             uint64_t nb = uint64_t(1) << (st->n - a.k);
             unsigned g = std::min<unsigned>(a.nslots, unsigned(ctx->num_sms) * 4);
@@ -482,6 +523,7 @@ double adjoint(qse_state* st, const qse_op* ops, size_t nops, const double* para
         }
     }
     for (uint32_t q = 0; q < st->n; ++q) st->perm[q] = pl.perm_final[q];
+    st->touch();
     std::vector<double> hocc(nops);
     QSE_CUDA(cudaMemcpyAsync(hocc.data(), occ, nops * 8, cudaMemcpyDeviceToHost, ctx->stream));
     QSE_CUDA(cudaStreamSynchronize(ctx->stream));

@@ -315,6 +315,7 @@ void launch_swap(qse_state* st, uint32_t q0, uint32_t q1)
 
 void launch_init_zero_state(qse_state* st)
 {
+    st->touch();
     QSE_CUDA(cudaMemsetAsync(st->amp, 0, st->size() * 16, st->ctx->stream));
     k_set_first<<<1, 1, 0, st->ctx->stream>>>(reinterpret_cast<double2*>(st->amp));
     QSE_CUDA(cudaGetLastError());

@@ -1,0 +1,483 @@
+// jit.cpp -- per-pass kernel specialisation.
+//
+// The planner lowers a pass into a short program (planner.h: KOp list,
+// register layouts, diagonal groups).  Interpreting that program per thread
+// costs more instructions than the arithmetic it drives.  Here each pass is
+// turned into straight-line CUDA C++ -- register positions, bit masks,
+// layouts, index offsets and conditions as compile-time constants; angles,
+// matrices and the pass scale as a __grid_constant__ parameter block -- and
+// compiled for sm_100a with NVRTC.  Kernels are cached by their source text,
+// so a circuit re-executed with new angles (parameter sweeps, gradients)
+// reuses them.  NVRTC is loaded with dlopen and the cubin through
+// cudaLibraryLoadData, so the library has no link-time dependency on either.
+#include "jit.h"
+
+#include <cuda_runtime.h>
+#include <dlfcn.h>
+#include <nvrtc.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <sstream>
+#include <thread>
+
+namespace qse {
+namespace jit {
+namespace {
+
+const char* kPrelude =
+#include "jit_prelude.inc"
+    ;
+
+// ---- NVRTC entry points (dlopen) ----
+struct Nvrtc {
+    decltype(&nvrtcCreateProgram) create = nullptr;
+    decltype(&nvrtcCompileProgram) compile = nullptr;
+    decltype(&nvrtcGetProgramLogSize) log_size = nullptr;
+    decltype(&nvrtcGetProgramLog) log = nullptr;
+    decltype(&nvrtcGetCUBINSize) cubin_size = nullptr;
+    decltype(&nvrtcGetCUBIN) cubin = nullptr;
+    decltype(&nvrtcDestroyProgram) destroy = nullptr;
+    decltype(&nvrtcGetErrorString) err = nullptr;
+    bool ok = false;
+    std::string why;
+};
+
+Nvrtc& nvrtc()
+{
+    static Nvrtc n;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        const char* names[] = {"libnvrtc.so.12", "libnvrtc.so", "/usr/local/cuda/lib64/libnvrtc.so.12",
+                               "/usr/local/cuda/lib64/libnvrtc.so"};
+        void* h = nullptr;
+        for (const char* nm : names)
+            if ((h = dlopen(nm, RTLD_NOW | RTLD_LOCAL))) break;
+        if (!h) {
+            n.why = "libnvrtc.so.12 not found";
+            return;
+        }
+#define QSE_SYM(field, name)                                                  \
+    n.field = reinterpret_cast<decltype(n.field)>(dlsym(h, name));            \
+    if (!n.field) {                                                           \
+        n.why = std::string("missing ") + name;                               \
+        return;                                                               \
+    }
+        QSE_SYM(create, "nvrtcCreateProgram");
+        QSE_SYM(compile, "nvrtcCompileProgram");
+        QSE_SYM(log_size, "nvrtcGetProgramLogSize");
+        QSE_SYM(log, "nvrtcGetProgramLog");
+        QSE_SYM(cubin_size, "nvrtcGetCUBINSize");
+        QSE_SYM(cubin, "nvrtcGetCUBIN");
+        QSE_SYM(destroy, "nvrtcDestroyProgram");
+        QSE_SYM(err, "nvrtcGetErrorString");
+#undef QSE_SYM
+        n.ok = true;
+    });
+    return n;
+}
+
+// ---- code generation ----
+struct Gen {
+    const plan::PassProgram& P;
+    int ns;
+    std::ostringstream o;
+    std::vector<double> prm;
+    uint32_t R, T, NW;
+    int reg[4];
+    int thr[16];
+    int nthr;
+
+    Gen(const plan::PassProgram& p, int nstates) : P(p), ns(nstates)
+    {
+        R = 1u << P.rb;
+        T = 1u << (P.k - P.rb);
+        NW = std::max(1u, T / 32);
+    }
+
+    void set_layout(const plan::LayoutRec& L)
+    {
+        for (uint32_t i = 0; i < P.rb; ++i) reg[i] = L.reg[i];
+        nthr = 0;
+        for (uint32_t b = 0; b < P.k; ++b) {
+            bool isreg = false;
+            for (uint32_t i = 0; i < P.rb; ++i) isreg |= reg[i] == int(b);
+            if (!isreg) thr[nthr++] = int(b);
+        }
+    }
+
+    static std::string hex(uint64_t v)
+    {
+        char b[32];
+        std::snprintf(b, sizeof(b), "0x%llxull", (unsigned long long)v);
+        return b;
+    }
+
+    // physical index of register 0 of this thread: outer base | thread bits deposited
+    std::string gbase_expr() const
+    {
+        std::string e = "ob";
+        for (int t = 0; t < nthr; ++t)
+            e += " | ((u64)((tid >> " + std::to_string(t) + ") & 1u) << " + std::to_string(P.tile_phys[thr[t]]) + ")";
+        return e;
+    }
+    uint64_t reg_off(uint32_t j) const
+    {
+        uint64_t off = 0;
+        for (uint32_t i = 0; i < P.rb; ++i)
+            if ((j >> i) & 1) off |= uint64_t(1) << P.tile_phys[reg[i]];
+        return off;
+    }
+    std::string slot_expr(const plan::LayoutRec& Lm) const
+    {
+        std::string e = "0u";
+        for (int t = 0; t < nthr; ++t)
+            e += " ^ (((tid >> " + std::to_string(t) + ") & 1u) * " + std::to_string(Lm.L[thr[t]]) + "u)";
+        return e;
+    }
+    uint32_t slot_off(const plan::LayoutRec& Lm, uint32_t j) const
+    {
+        uint32_t s = 0;
+        for (uint32_t i = 0; i < P.rb; ++i)
+            if ((j >> i) & 1) s ^= Lm.L[reg[i]];
+        return s;
+    }
+
+    uint32_t push(double v)
+    {
+        prm.push_back(v);
+        return uint32_t(prm.size() - 1);
+    }
+
+    std::string cond(uint16_t tcond, uint64_t ocond) const
+    {
+        std::string c;
+        if (tcond) c = "((tid & " + std::to_string(tcond) + "u) == " + std::to_string(tcond) + "u)";
+        if (ocond) {
+            if (!c.empty()) c += " && ";
+            c += "((ob & " + hex(ocond) + ") == " + hex(ocond) + ")";
+        }
+        return c;
+    }
+
+    void each_state(const std::string& stmt_with_A)
+    {
+        // stmt_with_A contains "A" for the register array of one state
+        for (int s = 0; s < ns; ++s) {
+            std::string st = stmt_with_A;
+            std::string name = s == 0 ? "a0" : "a1";
+            size_t pos = 0;
+            while ((pos = st.find("@A", pos)) != std::string::npos) {
+                st.replace(pos, 2, name);
+                pos += name.size();
+            }
+            o << "  " << st << "\n";
+        }
+    }
+
+    void emit_flush_reg(int p)
+    {
+        o << "  if (ar" << p << " != 0.0) { const double2 e = expi(ar" << p << "); ar" << p << " = 0.0;";
+        for (int s = 0; s < ns; ++s) o << " phD<" << (1 << p) << ">(" << (s ? "a1" : "a0") << ", e);";
+        o << " }\n";
+    }
+
+    std::string run()
+    {
+        const uint32_t tsize = 1u << P.k;
+        const uint32_t ng = uint32_t(P.groups.size());
+        const uint32_t nslots = uint32_t(P.slot_src.size());
+        std::ostringstream body;
+        std::swap(o, body);
+
+        o << "  const u32 tid = threadIdx.x;\n";
+        o << "  extern __shared__ double2 sm[];\n";
+        o << "  double2* xb = sm; (void)xb;\n";
+        o << "  double2* gv = sm + " << tsize << "; (void)gv;\n";
+        if (ns == 2) o << "  double* wp = reinterpret_cast<double*>(gv + " << ng << ");\n";
+        // outer base
+        o << "  u64 ob = 0;\n  { u64 c = blockIdx.x;";
+        for (uint32_t q = 0; q < 64; ++q)
+            if ((P.outer_mask >> q) & 1) o << " ob |= (c & 1ull) << " << q << "; c >>= 1;";
+        o << " (void)c; }\n";
+        // prologue: per-CTA diagonal group values
+        if (ng) {
+            o << "  for (u32 g = tid; g < " << ng << "u; g += " << T << "u) {\n"
+              << "    const GroupRec gr = groups[g]; double th = 0.0;\n"
+              << "    for (u32 i = 0; i < gr.count; ++i) { const TermRec t = terms[gr.first + i];"
+                 " if ((ob & t.ocond) == t.ocond) th += t.theta; }\n"
+              << "    gv[g] = gr.direct ? expi(th) : make_double2(th, 0.0);\n  }\n";
+        }
+        if (ns == 2 && nslots) o << "  for (u32 i = tid; i < " << nslots * NW << "u; i += " << T << "u) wp[i] = 0.0;\n";
+        o << "  __syncthreads();\n";
+        // load
+        set_layout(P.layouts[P.layout0]);
+        o << "  u64 gb = " << gbase_expr() << ";\n";
+        for (int s = 0; s < ns; ++s) o << "  double2 a" << s << "[" << R << "];\n";
+        for (uint32_t j = 0; j < R; ++j) {
+            o << "  a0[" << j << "] = psi[gb | " << hex(reg_off(j)) << "];";
+            if (ns == 2) o << " a1[" << j << "] = lam[gb | " << hex(reg_off(j)) << "];";
+            o << "\n";
+        }
+        o << "  double at = 0.0";
+        for (uint32_t i = 0; i < P.rb; ++i) o << ", ar" << i << " = 0.0";
+        o << ";\n";
+        for (uint32_t i = P.rb; i < 4; ++i) o << "  double ar" << i << " = 0.0; (void)ar" << i << ";\n";
+
+        for (const plan::KOp& op : P.ops) emit(op);
+
+        // store
+        for (uint32_t j = 0; j < R; ++j) {
+            o << "  psi[gb | " << hex(reg_off(j)) << "] = a0[" << j << "];";
+            if (ns == 2) o << " lam[gb | " << hex(reg_off(j)) << "] = a1[" << j << "];";
+            o << "\n";
+        }
+        if (ns == 2 && nslots) {
+            o << "  __syncthreads();\n"
+              << "  for (u32 s = tid; s < " << nslots << "u; s += " << T << "u) { double v = 0.0;"
+              << " for (u32 w = 0; w < " << NW << "u; ++w) v += wp[s * " << NW << "u + w];"
+              << " slot_partial[(u64)s * gridDim.x + blockIdx.x] = v; }\n";
+        }
+
+        std::swap(o, body);
+        std::ostringstream src;
+        src << kPrelude << "\n";
+        src << "struct Prm { double v[" << std::max<size_t>(1, prm.size()) << "]; };\n";
+        src << "extern \"C\" __global__ void __launch_bounds__(" << T << ", " << (T >= 64 ? 2 : 1) << ") qse_pass("
+            << "double2* __restrict__ psi, double2* __restrict__ lam, const TermRec* __restrict__ terms, "
+            << "const GroupRec* __restrict__ groups, double* __restrict__ slot_partial, const __grid_constant__ Prm P)\n{\n"
+            << "  (void)lam; (void)terms; (void)groups; (void)slot_partial;\n"
+            << body.str() << "}\n";
+        return src.str();
+    }
+
+    void emit(const plan::KOp& op)
+    {
+        using namespace plan;
+        const int p = op.p;
+        const std::string c = cond(op.tcond, op.ocond);
+        auto guarded = [&](const std::string& stmt) {
+            if (c.empty()) each_state(stmt);
+            else {
+                o << "  if (" << c << ") {\n";
+                each_state("  " + stmt);
+                o << "  }\n";
+            }
+        };
+        switch (op.kind) {
+        case K_H: each_state("opH<" + std::to_string(p) + ">(@A);"); break;
+        case K_X: guarded("opX<" + std::to_string(p) + ", " + std::to_string(op.f) + ">(@A);"); break;
+        case K_Y: guarded("opY<" + std::to_string(p) + ", " + std::to_string(op.f) + ">(@A);"); break;
+        case K_RX: case K_RY: {
+            uint32_t i = push(op.a);
+            push(op.b);
+            each_state(std::string(op.kind == K_RX ? "opRX<" : "opRY<") + std::to_string(p) + ">(@A, P.v[" +
+                       std::to_string(i) + "], P.v[" + std::to_string(i + 1) + "]);");
+            break;
+        }
+        case K_U: {
+            uint32_t i = uint32_t(prm.size());
+            for (int t = 0; t < 8; ++t) push(P.mats[8 * op.g + t]);
+            guarded("opU<" + std::to_string(p) + ", " + std::to_string(op.f) + ">(@A, &P.v[" + std::to_string(i) + "]);");
+            break;
+        }
+        case K_ACC_THR:
+            o << "  " << (op.tcond ? "if (" + cond(op.tcond, 0) + ") " : std::string()) << "at += gv[" << op.g
+              << "].x;\n";
+            break;
+        case K_ACC_REG:
+            o << "  " << (op.tcond ? "if (" + cond(op.tcond, 0) + ") " : std::string()) << "ar" << p << " += gv["
+              << op.g << "].x;\n";
+            break;
+        case K_PHD: {
+            std::string t = op.tcond ? "if (" + cond(op.tcond, 0) + ") " : std::string();
+            o << "  " << t << "{ const double2 e = gv[" << op.g << "];";
+            for (int s = 0; s < ns; ++s) o << " phD<" << int(op.f) << ">(" << (s ? "a1" : "a0") << ", e);";
+            o << " }\n";
+            break;
+        }
+        case K_FLUSH_REG: emit_flush_reg(p); break;
+        case K_FLUSH_ALL: {
+            for (uint32_t r = 0; r < P.rb; ++r)
+                if ((op.f >> r) & 1) emit_flush_reg(int(r));
+            const bool unit = op.a == 1.0 && op.b == 0.0;
+            if (unit) {
+                o << "  if (at != 0.0) { const double2 e = expi(at); at = 0.0;";
+            } else {
+                uint32_t i = push(op.a);
+                push(op.b);
+                o << "  { double2 e = make_double2(P.v[" << i << "], P.v[" << i + 1 << "]);"
+                  << " if (at != 0.0) { e = cmul(e, expi(at)); at = 0.0; }";
+            }
+            for (int s = 0; s < ns; ++s) o << " scaleAll(" << (s ? "a1" : "a0") << ", e);";
+            o << " }\n";
+            break;
+        }
+        case K_TRANSPOSE: {
+            const LayoutRec& nl = P.layouts[op.g];
+            o << "  {\n    const u32 sw = " << slot_expr(nl) << ";\n";
+            uint32_t woff[16];
+            for (uint32_t j = 0; j < R; ++j) woff[j] = slot_off(nl, j);
+            set_layout(nl);
+            o << "    const u32 sr = " << slot_expr(nl) << ";\n";
+            for (int s = 0; s < ns; ++s) {
+                const char* A = s ? "a1" : "a0";
+                o << "    __syncthreads();\n";
+                for (uint32_t j = 0; j < R; ++j) o << "    xb[sw ^ " << woff[j] << "u] = " << A << "[" << j << "];\n";
+                o << "    __syncthreads();\n";
+                for (uint32_t j = 0; j < R; ++j)
+                    o << "    " << A << "[" << j << "] = xb[sr ^ " << slot_off(nl, j) << "u];\n";
+            }
+            o << "    gb = " << gbase_expr() << ";\n  }\n";
+            break;
+        }
+        case K_GRAD_X: case K_GRAD_Y: case K_GRAD_Z: case K_GRAD_P: {
+            if (ns != 2) break;
+            std::string expr;
+            if (op.kind == K_GRAD_X) expr = "gradX<" + std::to_string(p) + ">(a0, a1)";
+            else if (op.kind == K_GRAD_Y) expr = "gradY<" + std::to_string(p) + ">(a0, a1)";
+            else if (op.kind == K_GRAD_Z) {
+                expr = "gradZ<" + std::to_string(p < int(P.rb) ? p : -1) + ">(a0, a1)";
+                std::string sg;
+                if (op.tcond) sg += "((tid & " + std::to_string(op.tcond) + "u) != 0u)";
+                if (op.ocond) sg += std::string(sg.empty() ? "" : " != ") + "((ob & " + hex(op.ocond) + ") != 0ull)";
+                if (!sg.empty()) expr = "((" + sg + ") ? -" + expr + " : " + expr + ")";
+            } else {
+                expr = "gradP<" + std::to_string(int(op.f)) + ">(a0, a1)";
+                if (!c.empty()) expr = "((" + c + ") ? " + expr + " : 0.0)";
+            }
+            const uint32_t si = push(op.a);
+            o << "  { const double v = warpSum<" << T << ">(" << expr << " * P.v[" << si << "]);"
+              << " if ((tid & 31u) == 0u) wp[" << op.g << "u * " << NW << "u + (tid >> 5)] += v; }\n";
+            break;
+        }
+        default: break;
+        }
+    }
+};
+
+std::mutex g_mu;
+std::map<std::string, std::shared_ptr<Kernel>> g_cache;
+
+std::string compile_to_cubin(const std::string& src, std::string& err)
+{
+    Nvrtc& nv = nvrtc();
+    nvrtcProgram prog;
+    if (nv.create(&prog, src.c_str(), "qse_pass.cu", 0, nullptr, nullptr) != NVRTC_SUCCESS) {
+        err = "nvrtcCreateProgram failed";
+        return {};
+    }
+    const char* opts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "-default-device", "--restrict"};
+    nvrtcResult r = nv.compile(prog, 4, opts);
+    if (r != NVRTC_SUCCESS) {
+        size_t n = 0;
+        nv.log_size(prog, &n);
+        std::string log(n, '\0');
+        if (n) nv.log(prog, &log[0]);
+        err = std::string("NVRTC: ") + nv.err(r) + "\n" + log;
+        nv.destroy(&prog);
+        return {};
+    }
+    size_t n = 0;
+    nv.cubin_size(prog, &n);
+    std::string bin(n, '\0');
+    nv.cubin(prog, &bin[0]);
+    nv.destroy(&prog);
+    return bin;
+}
+
+}  // namespace
+
+size_t compile_only(const Source& s)
+{
+    if (!available(nullptr)) fail(QSE_ERR_UNSUPPORTED, "NVRTC unavailable: " + nvrtc().why);
+    std::string err;
+    std::string bin = compile_to_cubin(s.code, err);
+    if (bin.empty()) fail(QSE_ERR_CUDA, "pass kernel compilation failed: " + err);
+    return bin.size();
+}
+
+bool available(std::string* why)
+{
+    Nvrtc& nv = nvrtc();
+    if (!nv.ok && why) *why = nv.why;
+    return nv.ok;
+}
+
+Source generate(const plan::PassProgram& p, int nstates)
+{
+    Gen g(p, nstates);
+    Source s;
+    s.code = g.run();
+    s.prm = std::move(g.prm);
+    s.threads = g.T;
+    s.smem = (size_t(1) << p.k) * 16 + p.groups.size() * 16 +
+             (nstates == 2 ? p.slot_src.size() * g.NW * 8 : 0);
+    return s;
+}
+
+std::vector<std::shared_ptr<Kernel>> get_kernels(const std::vector<const Source*>& srcs)
+{
+    std::vector<std::shared_ptr<Kernel>> out(srcs.size());
+    std::vector<size_t> missing;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        for (size_t i = 0; i < srcs.size(); ++i) {
+            auto it = g_cache.find(srcs[i]->code);
+            if (it != g_cache.end()) out[i] = it->second;
+            else missing.push_back(i);
+        }
+    }
+    if (missing.empty()) return out;
+    if (!available(nullptr)) fail(QSE_ERR_UNSUPPORTED, "NVRTC unavailable: " + nvrtc().why);
+    // distinct sources only, compiled in parallel
+    std::map<std::string, size_t> uniq;
+    std::vector<size_t> todo;
+    for (size_t i : missing)
+        if (uniq.emplace(srcs[i]->code, i).second) todo.push_back(i);
+    std::vector<std::string> bins(todo.size()), errs(todo.size());
+    const size_t nth = std::min<size_t>(todo.size(), std::max(1u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    std::atomic<size_t> next{0};
+    for (size_t t = 0; t < nth; ++t)
+        pool.emplace_back([&] {
+            for (size_t w; (w = next.fetch_add(1)) < todo.size();) bins[w] = compile_to_cubin(srcs[todo[w]]->code, errs[w]);
+        });
+    for (auto& th : pool) th.join();
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (size_t w = 0; w < todo.size(); ++w) {
+        if (bins[w].empty()) fail(QSE_ERR_CUDA, "pass kernel compilation failed: " + errs[w]);
+        auto k = std::make_shared<Kernel>();
+        QSE_CUDA(cudaLibraryLoadData(&k->lib, bins[w].data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+        QSE_CUDA(cudaLibraryGetKernel(&k->kern, k->lib, "qse_pass"));
+        k->threads = srcs[todo[w]]->threads;
+        g_cache[srcs[todo[w]]->code] = k;
+    }
+    for (size_t i : missing) out[i] = g_cache[srcs[i]->code];
+    return out;
+}
+
+void launch(qse_ctx* ctx, Kernel& k, const Source& s, uint32_t n, uint32_t kq, void* psi, void* lam,
+            const void* terms, const void* groups, double* slot_partial)
+{
+    if (s.smem > ctx->smem_optin) fail(QSE_ERR_SIZE, "pass needs more shared memory than the device offers");
+    if (s.smem > k.smem_set) {
+        QSE_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(k.kern), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(s.smem)));
+        k.smem_set = s.smem;
+    }
+    std::vector<double> prm = s.prm;
+    if (prm.empty()) prm.push_back(0.0);
+    void* args[] = {&psi, &lam, const_cast<const void**>(&terms), const_cast<const void**>(&groups), &slot_partial,
+                    prm.data()};
+    const uint64_t grid = uint64_t(1) << (n - kq);
+    QSE_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(k.kern), dim3(unsigned(grid)), dim3(k.threads), args,
+                              s.smem, ctx->stream));
+}
+
+}  // namespace jit
+}  // namespace qse

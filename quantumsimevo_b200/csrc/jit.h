@@ -1,0 +1,41 @@
+// jit.h -- per-pass kernel specialisation with NVRTC (jit.cpp).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "planner.h"
+#include "qse_internal.h"
+
+namespace qse {
+namespace jit {
+
+struct Source {
+    std::string code;         // CUDA C++ of the pass kernel (angles not included)
+    std::vector<double> prm;  // the kernel's parameter block (angles, matrices, scales)
+    uint32_t threads = 0;
+    size_t smem = 0;
+};
+
+struct Kernel {
+    cudaLibrary_t lib = nullptr;
+    cudaKernel_t kern = nullptr;
+    uint32_t threads = 0;
+    size_t smem_set = 48 * 1024;
+};
+
+bool available(std::string* why);
+// compiles one source without loading it (no GPU needed); returns the cubin size
+size_t compile_only(const Source& s);
+Source generate(const plan::PassProgram& p, int nstates);
+// compiled kernels for every source (cached by source text; missing ones are compiled in parallel)
+std::vector<std::shared_ptr<Kernel>> get_kernels(const std::vector<const Source*>& srcs);
+void launch(qse_ctx* ctx, Kernel& k, const Source& s, uint32_t n, uint32_t kq, void* psi, void* lam,
+            const void* terms, const void* groups, double* slot_partial);
+
+}  // namespace jit
+}  // namespace qse

@@ -52,6 +52,7 @@ struct qse_ctx {
     cudaStream_t stream = nullptr;
     // planner knobs
     int fusion = 1;
+    int jit = 1;             // specialised NVRTC pass kernels (0: generic interpreter kernel)
     int tile_qubits = 12;
     int max_gates_per_pass = 0;
     int sample_mode = 0;
@@ -64,6 +65,11 @@ struct qse_ctx {
     qse::HostBuf host_small; // pinned small results
     qse::HostBuf host_small2;
     cudaEvent_t plan_event = nullptr;  // last H2D copy out of plan_host
+    cudaEvent_t slots[64] = {};        // qse_ctx_record / qse_ctx_elapsed
+    // qse_ctx_time_passes: event pairs around every fused-pass launch
+    bool time_passes = false;
+    std::vector<cudaEvent_t> pass_events;  // pool, pairs (start, stop)
+    size_t pass_events_used = 0;
 };
 
 struct qse_state {
@@ -72,6 +78,15 @@ struct qse_state {
     double* amp = nullptr;       // 2^n complex128 (interleaved), physical qubit order
     double* aux = nullptr;       // second state (adjoint |lambda>), allocated on first use
     uint32_t perm[64];           // logical qubit -> physical bit
+    uint64_t version = 0;        // bumped by every call that writes the amplitudes
+    // exact cumulative probabilities (sample.cu), valid while cdf_version == version
+    qse::DevBuf cdf;
+    uint64_t cdf_version = ~uint64_t(0);
+    double* cdf_values = nullptr;
+    double* cdf_block_start = nullptr;
+    uint32_t cdf_nb = 0;
+    uint32_t cdf_bs = 0;
+    void touch() { ++version; }
     bool identity_perm() const {
         for (uint32_t q = 0; q < n; ++q)
             if (perm[q] != q) return false;
@@ -121,6 +136,7 @@ void canonicalize(qse_state* st);
 
 // ---- sampling (sample.cu) ----
 void sample(qse_state* st, const double* u_host, size_t nshots, uint64_t seed, uint64_t* out_host);
+void sample_device(qse_state* st, const double* d_u, size_t nshots, uint64_t seed, uint64_t* d_out);
 uint64_t measure(qse_state* st, double u);
 double total_probability(qse_state* st);
 

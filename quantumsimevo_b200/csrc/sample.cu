@@ -322,34 +322,62 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double2* __restrict__ a
     __shared__ uint64_t sh[160];
     __shared__ double s_c;
     __shared__ int s_slow;
-    if (threadIdx.x == 0) s_c = 0.0;
+    const uint32_t t = threadIdx.x;
+    if (t == 0) s_c = 0.0;
     __syncthreads();
-    for (uint32_t b = 0; b < nb; ++b) {
-        if (threadIdx.x == 0) {
-            double c = s_c;
-            cin[b] = c;
-            Summ s = summ[b];
-            int slow = 1;
-            if (s.ok && s.e != INT32_MIN && c > 0.0 && epoch_of(c) == s.e) {
-                uint64_t C = uint64_t(ldexp(c, 52 - s.e));
-                uint64_t Co = C + ((C & 1) ? s.d1 : s.d0);
-                if (Co < kTwo53 && Co >= C) {
-                    s_c = ldexp(double(Co), s.e - 52);
-                    slow = 0;
+    // Chunks of kBT consecutive blocks.  When every block of the chunk was
+    // folded on the grid of the running sum's binade, the chunk's maps compose
+    // with one block-wide scan; if the sum stays inside the binade to the end
+    // of the chunk, every block start is exact.  Otherwise the chunk is walked
+    // block by block (blocks that fail are folded exactly).
+    for (uint32_t base = 0; base < nb; base += kBT) {
+        const uint32_t cnt = min(uint32_t(kBT), nb - base);
+        const double c = s_c;
+        const int e0 = epoch_of(c);
+        Summ s{0, 0, e0, 1};
+        if (t < cnt) s = summ[base + t];
+        const bool good = (t >= cnt) || (s.ok && s.e == e0 && c > 0.0);
+        bool fast = __syncthreads_and(good) != 0;
+        uint64_t ex0 = 0, ex1 = 0;
+        const uint64_t C = fast ? uint64_t(ldexp(c, 52 - e0)) : 0;
+        block_scan_maps(t < cnt ? s.d0 : 0, t < cnt ? s.d1 : 0, ex0, ex1, sh);
+        uint64_t cin_t = C + ((C & 1) ? ex1 : ex0);
+        uint64_t cout_t = cin_t + ((cin_t & 1) ? s.d1 : s.d0);
+        if (fast) fast = __syncthreads_and(t >= cnt || cout_t < kTwo53) != 0;
+        else __syncthreads();
+        if (fast) {
+            if (t < cnt) cin[base + t] = ldexp(double(cin_t), e0 - 52);
+            if (t == cnt - 1) s_c = ldexp(double(cout_t), e0 - 52);
+            __syncthreads();
+            continue;
+        }
+        for (uint32_t b = base; b < base + cnt; ++b) {
+            if (t == 0) {
+                double cc = s_c;
+                cin[b] = cc;
+                Summ sb = summ[b];
+                int slow = 1;
+                if (sb.ok && sb.e != INT32_MIN && cc > 0.0 && epoch_of(cc) == sb.e) {
+                    uint64_t Cb = uint64_t(ldexp(cc, 52 - sb.e));
+                    uint64_t Co = Cb + ((Cb & 1) ? sb.d1 : sb.d0);
+                    if (Co < kTwo53 && Co >= Cb) {
+                        s_c = ldexp(double(Co), sb.e - 52);
+                        slow = 0;
+                    }
                 }
+                s_slow = slow;
             }
-            s_slow = slow;
+            __syncthreads();
+            if (s_slow) {
+                double p[kEPT];
+                load_block_p(amp, uint64_t(b) * kBS, kBS, pm, p);
+                double cc = block_exact(p, kBS, s_c, nullptr, sh);
+                if (t == 0) s_c = cc;
+            }
+            __syncthreads();
         }
-        __syncthreads();
-        if (s_slow) {
-            double p[kEPT];
-            load_block_p(amp, uint64_t(b) * kBS, kBS, pm, p);
-            double c = block_exact(p, kBS, s_c, nullptr, sh);
-            if (threadIdx.x == 0) s_c = c;
-        }
-        __syncthreads();
     }
-    if (threadIdx.x == 0) cin[nb] = s_c;
+    if (t == 0) cin[nb] = s_c;
 }
 
 __global__ void __launch_bounds__(kBT) k_cdf_write(const double2* __restrict__ amp, PermMap pm,
@@ -437,47 +465,54 @@ struct CdfView {
     uint32_t bs;
 };
 
+// Exact cumulative array of the current amplitudes, cached per state until
+// the amplitudes change (sample() followed by measure() builds it once).
 CdfView build_cdf(qse_state* st)
 {
     qse_ctx* ctx = st->ctx;
     const uint64_t size = st->size();
+    if (st->cdf_version == st->version)
+        return CdfView{st->cdf_values, st->cdf_block_start, st->cdf_nb, st->cdf_bs};
     PermMap pm = make_perm(st);
     CdfView v{};
+    const double2* amp = reinterpret_cast<const double2*>(st->amp);
     if (size < uint64_t(kBS)) {
-        ctx->scratch2.reserve(size * 8 + 4 * 8);
-        v.cdf = static_cast<double*>(ctx->scratch2.ptr);
+        st->cdf.reserve(size * 8 + 4 * 8);
+        v.cdf = static_cast<double*>(st->cdf.ptr);
         v.cin = v.cdf + size;
         v.nb = 1;
         v.bs = uint32_t(size);
-        k_cdf_small<<<1, 32, 0, ctx->stream>>>(reinterpret_cast<const double2*>(st->amp), size, pm, v.cdf, v.cin);
+        k_cdf_small<<<1, 32, 0, ctx->stream>>>(amp, size, pm, v.cdf, v.cin);
         QSE_CUDA(cudaGetLastError());
         count_launch(ctx);
-        return v;
+    } else {
+        const uint32_t nb = uint32_t(size / kBS);
+        // state-owned: cdf [size] | cin [nb+1];  context scratch: bsum [nb] | guess [nb] | summ [nb]
+        st->cdf.reserve(size * 8 + (size_t(nb) + 1) * 8);
+        v.cdf = static_cast<double*>(st->cdf.ptr);
+        v.cin = v.cdf + size;
+        size_t off_guess = size_t(nb) * 8;
+        size_t off_summ = (off_guess + size_t(nb) * 4 + 15) & ~size_t(15);
+        ctx->scratch2.reserve(off_summ + size_t(nb) * sizeof(Summ));
+        char* base = static_cast<char*>(ctx->scratch2.ptr);
+        double* bsum = reinterpret_cast<double*>(base);
+        int32_t* guess = reinterpret_cast<int32_t*>(base + off_guess);
+        Summ* summ = reinterpret_cast<Summ*>(base + off_summ);
+        v.nb = nb;
+        v.bs = kBS;
+        k_cdf_bsum<<<nb, kBT, 0, ctx->stream>>>(amp, size, pm, bsum);
+        k_cdf_guess<<<1, 1024, 0, ctx->stream>>>(bsum, nb, guess);
+        k_cdf_summ<<<nb, kBT, 0, ctx->stream>>>(amp, pm, guess, summ);
+        k_cdf_chain<<<1, kBT, 0, ctx->stream>>>(amp, pm, summ, nb, v.cin);
+        k_cdf_write<<<nb, kBT, 0, ctx->stream>>>(amp, pm, v.cin, v.cdf);
+        QSE_CUDA(cudaGetLastError());
+        count_launch(ctx, 5);
     }
-    const uint32_t nb = uint32_t(size / kBS);
-    // scratch2: cdf [size] | cin [nb+1] | bsum [nb] | guess [nb] | summ [nb]
-    size_t off_cin = size * 8;
-    size_t off_bsum = off_cin + (size_t(nb) + 1) * 8;
-    size_t off_guess = off_bsum + size_t(nb) * 8;
-    size_t off_summ = (off_guess + size_t(nb) * 4 + 15) & ~size_t(15);
-    size_t total = off_summ + size_t(nb) * sizeof(Summ);
-    ctx->scratch2.reserve(total);
-    char* base = static_cast<char*>(ctx->scratch2.ptr);
-    v.cdf = reinterpret_cast<double*>(base);
-    v.cin = reinterpret_cast<double*>(base + off_cin);
-    double* bsum = reinterpret_cast<double*>(base + off_bsum);
-    int32_t* guess = reinterpret_cast<int32_t*>(base + off_guess);
-    Summ* summ = reinterpret_cast<Summ*>(base + off_summ);
-    v.nb = nb;
-    v.bs = kBS;
-    const double2* amp = reinterpret_cast<const double2*>(st->amp);
-    k_cdf_bsum<<<nb, kBT, 0, ctx->stream>>>(amp, size, pm, bsum);
-    k_cdf_guess<<<1, 1024, 0, ctx->stream>>>(bsum, nb, guess);
-    k_cdf_summ<<<nb, kBT, 0, ctx->stream>>>(amp, pm, guess, summ);
-    k_cdf_chain<<<1, kBT, 0, ctx->stream>>>(amp, pm, summ, nb, v.cin);
-    k_cdf_write<<<nb, kBT, 0, ctx->stream>>>(amp, pm, v.cin, v.cdf);
-    QSE_CUDA(cudaGetLastError());
-    count_launch(ctx, 5);
+    st->cdf_values = v.cdf;
+    st->cdf_block_start = v.cin;
+    st->cdf_nb = v.nb;
+    st->cdf_bs = v.bs;
+    st->cdf_version = st->version;
     return v;
 }
 
@@ -509,6 +544,18 @@ void sample(qse_state* st, const double* u_host, size_t nshots, uint64_t seed, u
     QSE_CUDA(cudaStreamSynchronize(ctx->stream));
 }
 
+void sample_device(qse_state* st, const double* d_u, size_t nshots, uint64_t seed, uint64_t* d_out)
+{
+    qse_ctx* ctx = st->ctx;
+    if (nshots == 0) return;
+    CdfView v = build_cdf(st);
+    unsigned grid = unsigned(std::min<uint64_t>((nshots + 255) / 256, uint64_t(ctx->num_sms) * 8));
+    k_sample<<<grid, 256, 0, ctx->stream>>>(v.cdf, st->size(), v.cin, v.nb, v.bs, d_u, nshots, seed, d_out,
+                                            make_perm(st));
+    QSE_CUDA(cudaGetLastError());
+    count_launch(ctx);
+}
+
 uint64_t measure(qse_state* st, double u)
 {
     uint64_t idx = 0;
@@ -520,6 +567,7 @@ uint64_t measure(qse_state* st, double u)
     uint64_t size = st->size();
     unsigned grid = unsigned(std::min<uint64_t>((size + 255) / 256, uint64_t(ctx->num_sms) * 32));
     k_collapse<<<grid, 256, 0, ctx->stream>>>(reinterpret_cast<double2*>(st->amp), size, P);
+    st->touch();
     QSE_CUDA(cudaGetLastError());
     count_launch(ctx);
     QSE_CUDA(cudaStreamSynchronize(ctx->stream));

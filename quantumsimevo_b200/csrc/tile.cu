@@ -521,12 +521,35 @@ void launch_t(qse_ctx* ctx, const PassArgs& a, uint32_t n, size_t smem)
     }
     uint32_t threads = 1u << (a.k - RB);
     uint64_t grid = uint64_t(1) << (n - a.k);
+    cudaEvent_t ev_stop = pass_timer_begin(ctx);
     k_tile<RB, NS><<<unsigned(grid), threads, smem, ctx->stream>>>(a);
     QSE_CUDA(cudaGetLastError());
+    pass_timer_end(ctx, ev_stop);
     count_launch(ctx);
 }
 
 }  // namespace
+
+cudaEvent_t pass_timer_begin(qse_ctx* ctx)
+{
+    if (!ctx->time_passes) return nullptr;
+    if (ctx->pass_events_used + 2 > ctx->pass_events.size()) {
+        for (int i = 0; i < 64; ++i) {
+            cudaEvent_t e;
+            QSE_CUDA(cudaEventCreate(&e));
+            ctx->pass_events.push_back(e);
+        }
+    }
+    QSE_CUDA(cudaEventRecord(ctx->pass_events[ctx->pass_events_used], ctx->stream));
+    cudaEvent_t stop = ctx->pass_events[ctx->pass_events_used + 1];
+    ctx->pass_events_used += 2;
+    return stop;
+}
+
+void pass_timer_end(qse_ctx* ctx, cudaEvent_t stop)
+{
+    if (stop) QSE_CUDA(cudaEventRecord(stop, ctx->stream));
+}
 
 size_t pass_smem_bytes(uint32_t k, uint32_t ngroups, uint32_t nslots, uint32_t rb, int nstates)
 {

@@ -31,6 +31,9 @@ struct PassArgs {
 // Launch one pass: grid = 2^(n-k) CTAs of 2^(k-rb) threads.
 void launch_pass(qse_ctx* ctx, const PassArgs& a, uint32_t n, uint32_t rb, int nstates);
 size_t pass_smem_bytes(uint32_t k, uint32_t ngroups, uint32_t nslots, uint32_t rb, int nstates);
+// events bracketing one pass launch when qse_ctx_time_passes is on (else no-ops)
+cudaEvent_t pass_timer_begin(qse_ctx* ctx);
+void pass_timer_end(qse_ctx* ctx, cudaEvent_t stop);
 
 }  // namespace tile
 }  // namespace qse
