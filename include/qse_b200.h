@@ -238,6 +238,10 @@ QSE_API int qse_sample_device(qse_state* st, const double* d_uniforms, size_t ns
                               uint64_t* d_out);
 /* measure(): outcome for uniform u, then collapse to |outcome> (amplitude 1, all others 0) */
 QSE_API int qse_measure(qse_state* st, double u, uint64_t* out_index);
+/* Diagnostics of the exact-CDF scan on the current state: out = {chunks composed
+ * in parallel, chunks walked block by block, blocks folded element by element,
+ * blocks}.  Rebuilds the cumulative array. */
+QSE_API int qse_sampler_stats(qse_state* st, uint32_t out[4]);
 /* total probability as the reference's sequential loop rounds it */
 QSE_API int qse_total_probability(qse_state* st, double* total);
 

@@ -583,6 +583,15 @@ int qse_measure(qse_state* st, double u, uint64_t* out_index)
     QSE_GUARD_END
 }
 
+int qse_sampler_stats(qse_state* st, uint32_t out[4])
+{
+    QSE_GUARD_BEGIN
+    need(st != nullptr && out != nullptr, QSE_ERR_INVALID, "null argument");
+    bind_device(st->ctx);
+    qse::sampler_stats(st, out);
+    QSE_GUARD_END
+}
+
 int qse_total_probability(qse_state* st, double* total)
 {
     QSE_GUARD_BEGIN

@@ -139,6 +139,7 @@ void sample(qse_state* st, const double* u_host, size_t nshots, uint64_t seed, u
 void sample_device(qse_state* st, const double* d_u, size_t nshots, uint64_t seed, uint64_t* d_out);
 uint64_t measure(qse_state* st, double u);
 double total_probability(qse_state* st);
+void sampler_stats(qse_state* st, uint32_t out[4]);
 
 // ---- noise (noise.cu) ----
 void noise_decide(qse_noise* nz, const int32_t* d_types, const uint32_t* d_targets, size_t ngates,

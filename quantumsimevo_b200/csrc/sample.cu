@@ -38,11 +38,26 @@ constexpr int kEPT = 16;            // elements per thread
 constexpr int kBS = kBT * kEPT;     // elements per block (4096)
 constexpr uint64_t kTwo53 = uint64_t(1) << 53;
 
-struct Summ {                       // block fold on a guessed grid
-    uint64_t d0, d1;                // offsets for even / odd incoming sum
-    int32_t e;                      // grid exponent guessed (INT32_MIN: no guess)
-    int32_t ok;                     // 0: a step may leave the binade
+// Block folds on the grids of two adjacent binades, e and e+1: the running sum
+// at the block is known only approximately, and near a binade boundary (for a
+// normalised state the sum ends just below 1.0 = 2^0 for many blocks) either
+// can hold.  The chain picks the fold of the binade the exact sum is in.
+struct Summ {
+    uint64_t d[2][2];               // d[k] = offsets (even, odd incoming sum) on the grid of binade e+k
+    int32_t e;                      // lower binade guessed (INT32_MIN: no guess)
+    int32_t ok;                     // bit k: no single step leaves binade e+k
 };
+
+// the fold of s that applies to a running sum in binade e0, if any
+__device__ __forceinline__ bool summ_pick(const Summ& s, int e0, uint64_t& d0, uint64_t& d1)
+{
+    if (s.e == INT32_MIN) return false;
+    const int k = e0 - s.e;
+    if (k < 0 || k > 1 || !((s.ok >> k) & 1)) return false;
+    d0 = s.d[k][0];
+    d1 = s.d[k][1];
+    return true;
+}
 
 __device__ __forceinline__ double norm2(double2 a)
 {
@@ -278,7 +293,7 @@ __global__ void __launch_bounds__(1024) k_cdf_guess(const double* __restrict__ b
         double slack = hi_c * 0x1.0p-20 + 1e-300;
         int e1 = lo_c - slack > 2.2250738585072014e-308 ? ilogb(lo_c - slack) : -1022;
         int e2 = hi_c + slack > 2.2250738585072014e-308 ? ilogb(hi_c + slack) : -1022;
-        guess[b] = (e1 == e2) ? e1 : INT32_MIN;
+        guess[b] = (e2 - e1 <= 1) ? e1 : INT32_MIN;
         run = hi_c;
     }
 }
@@ -289,79 +304,99 @@ __global__ void __launch_bounds__(kBT) k_cdf_summ(const double2* __restrict__ am
     __shared__ uint64_t sh[160];
     const int32_t e = guess[blockIdx.x];
     if (e == INT32_MIN) {
-        if (threadIdx.x == 0) summ[blockIdx.x] = Summ{0, 0, e, 0};
+        if (threadIdx.x == 0) summ[blockIdx.x] = Summ{{{0, 0}, {0, 0}}, e, 0};
         return;
     }
     double p[kEPT];
     load_block_p(amp, uint64_t(blockIdx.x) * kBS, kBS, pm, p);
-    uint64_t t0 = 0, t1 = 0;
-    int ok = 1;
+    Summ out{{{0, 0}, {0, 0}}, e, 0};
+    for (int k = 0; k < 2; ++k) {
+        uint64_t t0 = 0, t1 = 0;
+        int ok = 1;
 #pragma unroll
-    for (int j = 0; j < kEPT; ++j) {
-        uint64_t a0, a1, r0, r1;
-        if (!elem_map(p[j], e, a0, a1)) ok = 0;
-        compose(t0, t1, a0, a1, r0, r1);
-        t0 = r0;
-        t1 = r1;
-    }
-    ok = __syncthreads_and(ok);
-    uint64_t ex0, ex1;
-    block_scan_maps(t0, t1, ex0, ex1, sh);
-    if (threadIdx.x == blockDim.x - 1) {
+        for (int j = 0; j < kEPT; ++j) {
+            uint64_t a0, a1, r0, r1;
+            if (!elem_map(p[j], e + k, a0, a1)) ok = 0;
+            compose(t0, t1, a0, a1, r0, r1);
+            t0 = r0;
+            t1 = r1;
+        }
+        ok = __syncthreads_and(ok);
+        uint64_t ex0, ex1;
+        block_scan_maps(t0, t1, ex0, ex1, sh);
         uint64_t r0, r1;
         compose(ex0, ex1, t0, t1, r0, r1);
-        summ[blockIdx.x] = Summ{r0, r1, e, ok};
+        out.d[k][0] = r0;
+        out.d[k][1] = r1;
+        out.ok |= ok ? (1 << k) : 0;
     }
+    if (threadIdx.x == blockDim.x - 1) summ[blockIdx.x] = out;
 }
 
 // single CTA: exact running sum block by block; blocks whose guess does not
 // hold are folded exactly here.  cin[b] = exact sum before block b; cin[nb] = total.
 __global__ void __launch_bounds__(kBT) k_cdf_chain(const double2* __restrict__ amp, PermMap pm,
-                                                   const Summ* __restrict__ summ, uint32_t nb, double* __restrict__ cin)
+                                                   const Summ* __restrict__ summ, uint32_t nb, double* __restrict__ cin,
+                                                   uint32_t* __restrict__ stats)
 {
     __shared__ uint64_t sh[160];
+    uint32_t n_fast = 0, n_slow = 0, n_exact = 0;  // chunk / block statistics (thread 0)
     __shared__ double s_c;
     __shared__ int s_slow;
     const uint32_t t = threadIdx.x;
     if (t == 0) s_c = 0.0;
     __syncthreads();
-    // Chunks of kBT consecutive blocks.  When every block of the chunk was
-    // folded on the grid of the running sum's binade, the chunk's maps compose
-    // with one block-wide scan; if the sum stays inside the binade to the end
-    // of the chunk, every block start is exact.  Otherwise the chunk is walked
-    // block by block (blocks that fail are folded exactly).
+    // Chunks of kBT consecutive blocks.  From position pos, the blocks whose
+    // fold exists on the grid of the running sum's binade compose with one
+    // block-wide scan up to the first block that has no such fold or whose
+    // sum leaves the binade; that block is handled on its own (its fold on
+    // the binade it actually starts in, else an exact element-by-element
+    // fold) and the scan restarts after it.
+    __shared__ int s_end;
     for (uint32_t base = 0; base < nb; base += kBT) {
         const uint32_t cnt = min(uint32_t(kBT), nb - base);
-        const double c = s_c;
-        const int e0 = epoch_of(c);
-        Summ s{0, 0, e0, 1};
-        if (t < cnt) s = summ[base + t];
-        const bool good = (t >= cnt) || (s.ok && s.e == e0 && c > 0.0);
-        bool fast = __syncthreads_and(good) != 0;
-        uint64_t ex0 = 0, ex1 = 0;
-        const uint64_t C = fast ? uint64_t(ldexp(c, 52 - e0)) : 0;
-        block_scan_maps(t < cnt ? s.d0 : 0, t < cnt ? s.d1 : 0, ex0, ex1, sh);
-        uint64_t cin_t = C + ((C & 1) ? ex1 : ex0);
-        uint64_t cout_t = cin_t + ((cin_t & 1) ? s.d1 : s.d0);
-        if (fast) fast = __syncthreads_and(t >= cnt || cout_t < kTwo53) != 0;
-        else __syncthreads();
-        if (fast) {
-            if (t < cnt) cin[base + t] = ldexp(double(cin_t), e0 - 52);
-            if (t == cnt - 1) s_c = ldexp(double(cout_t), e0 - 52);
+        uint32_t pos = 0;
+        while (pos < cnt) {
+            const double c = s_c;
+            const int e0 = epoch_of(c);
+            uint64_t m0 = 0, m1 = 0;
+            bool good = true;
+            if (t >= pos && t < cnt) good = c > 0.0 && summ_pick(summ[base + t], e0, m0, m1);
+            if (t == 0) s_end = int(cnt);
             __syncthreads();
-            continue;
-        }
-        for (uint32_t b = base; b < base + cnt; ++b) {
+            if (!good) atomicMin(&s_end, int(t));
+            __syncthreads();
+            const uint32_t bad = uint32_t(s_end);
+            if (t >= bad) m0 = m1 = 0;
+            uint64_t ex0, ex1;
+            block_scan_maps(m0, m1, ex0, ex1, sh);
+            const uint64_t C = c > 0.0 ? uint64_t(ldexp(c, 52 - e0)) : 0;
+            const uint64_t cin_t = C + ((C & 1) ? ex1 : ex0);
+            const uint64_t cout_t = cin_t + ((cin_t & 1) ? m1 : m0);
+            if (t == 0) s_end = int(bad);
+            __syncthreads();
+            if (t >= pos && t < bad && cout_t >= kTwo53) atomicMin(&s_end, int(t));
+            __syncthreads();
+            const uint32_t end = uint32_t(s_end);
+            if (t >= pos && t < end) cin[base + t] = ldexp(double(cin_t), e0 - 52);
+            if (end > pos && t == end - 1) s_c = ldexp(double(cout_t), e0 - 52);
+            if (end > pos) ++n_fast;
+            __syncthreads();
+            if (end >= cnt) break;
+            ++n_slow;
+            const uint32_t b = base + end;
+            pos = end + 1;
             if (t == 0) {
                 double cc = s_c;
                 cin[b] = cc;
-                Summ sb = summ[b];
+                const int eb = epoch_of(cc);
+                uint64_t b0, b1;
                 int slow = 1;
-                if (sb.ok && sb.e != INT32_MIN && cc > 0.0 && epoch_of(cc) == sb.e) {
-                    uint64_t Cb = uint64_t(ldexp(cc, 52 - sb.e));
-                    uint64_t Co = Cb + ((Cb & 1) ? sb.d1 : sb.d0);
+                if (cc > 0.0 && summ_pick(summ[b], eb, b0, b1)) {
+                    uint64_t Cb = uint64_t(ldexp(cc, 52 - eb));
+                    uint64_t Co = Cb + ((Cb & 1) ? b1 : b0);
                     if (Co < kTwo53 && Co >= Cb) {
-                        s_c = ldexp(double(Co), sb.e - 52);
+                        s_c = ldexp(double(Co), eb - 52);
                         slow = 0;
                     }
                 }
@@ -369,6 +404,7 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double2* __restrict__ a
             }
             __syncthreads();
             if (s_slow) {
+                ++n_exact;
                 double p[kEPT];
                 load_block_p(amp, uint64_t(b) * kBS, kBS, pm, p);
                 double cc = block_exact(p, kBS, s_c, nullptr, sh);
@@ -377,7 +413,15 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double2* __restrict__ a
             __syncthreads();
         }
     }
-    if (t == 0) cin[nb] = s_c;
+    if (t == 0) {
+        cin[nb] = s_c;
+        if (stats) {
+            stats[0] = n_fast;
+            stats[1] = n_slow;
+            stats[2] = n_exact;
+            stats[3] = nb;
+        }
+    }
 }
 
 __global__ void __launch_bounds__(kBT) k_cdf_write(const double2* __restrict__ amp, PermMap pm,
@@ -488,7 +532,7 @@ CdfView build_cdf(qse_state* st)
     } else {
         const uint32_t nb = uint32_t(size / kBS);
         // state-owned: cdf [size] | cin [nb+1];  context scratch: bsum [nb] | guess [nb] | summ [nb]
-        st->cdf.reserve(size * 8 + (size_t(nb) + 1) * 8);
+        st->cdf.reserve(size * 8 + (size_t(nb) + 1) * 8 + 16);
         v.cdf = static_cast<double*>(st->cdf.ptr);
         v.cin = v.cdf + size;
         size_t off_guess = size_t(nb) * 8;
@@ -503,7 +547,8 @@ CdfView build_cdf(qse_state* st)
         k_cdf_bsum<<<nb, kBT, 0, ctx->stream>>>(amp, size, pm, bsum);
         k_cdf_guess<<<1, 1024, 0, ctx->stream>>>(bsum, nb, guess);
         k_cdf_summ<<<nb, kBT, 0, ctx->stream>>>(amp, pm, guess, summ);
-        k_cdf_chain<<<1, kBT, 0, ctx->stream>>>(amp, pm, summ, nb, v.cin);
+        k_cdf_chain<<<1, kBT, 0, ctx->stream>>>(amp, pm, summ, nb, v.cin,
+                                                reinterpret_cast<uint32_t*>(v.cin + nb + 1));
         k_cdf_write<<<nb, kBT, 0, ctx->stream>>>(amp, pm, v.cin, v.cdf);
         QSE_CUDA(cudaGetLastError());
         count_launch(ctx, 5);
@@ -583,4 +628,18 @@ double total_probability(qse_state* st)
     return t;
 }
 
+}  // namespace qse
+
+namespace qse {
+// chain statistics of the last exact-CDF build of st: fast chunks, slow
+// chunks, blocks folded exactly, blocks (zeros for states below one block)
+void sampler_stats(qse_state* st, uint32_t out[4])
+{
+    st->cdf_version = ~uint64_t(0);
+    CdfView v = build_cdf(st);
+    std::memset(out, 0, 16);
+    if (v.nb > 1 || st->size() >= uint64_t(kBS))
+        QSE_CUDA(cudaMemcpyAsync(out, v.cin + v.nb + 1, 16, cudaMemcpyDeviceToHost, st->ctx->stream));
+    QSE_CUDA(cudaStreamSynchronize(st->ctx->stream));
+}
 }  // namespace qse
