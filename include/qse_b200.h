@@ -248,6 +248,15 @@ QSE_API int qse_total_probability(qse_state* st, double* total);
 /* ---- differentiation (no reference counterpart) ---- */
 /* <psi|O|psi> for the current state */
 QSE_API int qse_expectation(qse_state* st, const qse_observable* obs, double* value);
+/* <psi|O|psi> like qse_expectation, for callers that cannot allocate memory at
+ * the point of the call (a locked or exhausted allocator, an embedding that
+ * forbids allocation after start-up).  It allocates nothing, device or host:
+ * its scratch is a fixed 64 KiB device array inside the library, so it takes
+ * at most 2048 observable terms (more: QSE_ERR_SIZE).  All calls on a device
+ * share that array, so calls that overlap on the GPU race; the first call on
+ * a device looks up the array's address and should come before any stream
+ * capture.  No counterpart in the reference (it has no observables). */
+QSE_API int qse_expectation_noalloc(qse_state* st, const qse_observable* obs, double* value);
 /* Runs ops from |0..0> into st, then the adjoint sweep: grad[p] = d<O>/d params[p].
  * Parameterised types: RX, RY, RZ, PHASE, CPHASE, MCPHASE. */
 QSE_API int qse_adjoint(qse_state* st, const qse_op* ops, size_t nops,

@@ -198,6 +198,7 @@ def default_noise_config(enabled=True, rng_mode=RNG_PHILOX, seed=42, multiplier=
 for _name, (_args, _res) in {
     "qse_ctx_set_jit": ([_vp, C.c_int], C.c_int),
     "qse_sampler_stats": ([_vp, C.POINTER(_u32)], C.c_int),
+    "qse_expectation_noalloc": ([_vp, C.POINTER(QseObservable), _pd], C.c_int),
     "qse_plan_compile": ([_u32, _vp, _sz, _pd, _sz, _u32, C.c_int, C.POINTER(_sz)], C.c_int),
 }.items():
     _f = getattr(lib, _name)

@@ -611,6 +611,16 @@ int qse_expectation(qse_state* st, const qse_observable* obs, double* value)
     QSE_GUARD_END
 }
 
+int qse_expectation_noalloc(qse_state* st, const qse_observable* obs, double* value)
+{
+    QSE_GUARD_BEGIN
+    need(st && obs && value, QSE_ERR_INVALID, "null argument");
+    need(obs->nterms == 0 || (obs->zmask && obs->weight), QSE_ERR_INVALID, "null observable terms");
+    bind_device(st->ctx);
+    *value = qse::expectation_noalloc(st, obs);
+    QSE_GUARD_END
+}
+
 int qse_adjoint(qse_state* st, const qse_op* ops, size_t nops, const double* params, size_t nparams,
                 const qse_observable* obs, double* value, double* grad)
 {

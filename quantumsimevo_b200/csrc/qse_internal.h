@@ -146,6 +146,7 @@ void noise_decide(qse_noise* nz, const int32_t* d_types, const uint32_t* d_targe
                   const double* d_uniforms);
 // ---- observables / adjoint (adjoint.cu) ----
 double expectation(qse_state* st, const qse_observable* obs);
+double expectation_noalloc(qse_state* st, const qse_observable* obs);
 double adjoint(qse_state* st, const qse_op* ops, size_t nops, const double* params, size_t nparams,
                const qse_observable* obs, double* grad);
 
