@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--no-qaoa", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-gates", type=int, default=0, help="gates in the CPU sample (0 = auto)")
+    ap.add_argument("--tile", type=int, default=0, help="tile qubits of the fused passes (0 = library default)")
     return ap.parse_args()
 
 
@@ -222,6 +223,8 @@ def main():
     ops = W.hrz_qft(n, seed=2)
     ngates = len(ops)
     dev = Device(local)
+    if args.tile:
+        dev.set_fusion(True, args.tile, 0)
     lib = L.lib
     st = StateVector(n, dev)
     d_out = C.c_void_p()

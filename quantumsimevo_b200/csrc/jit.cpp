@@ -247,7 +247,9 @@ struct Gen {
         std::ostringstream src;
         src << kPrelude << "\n";
         src << "struct Prm { double v[" << std::max<size_t>(1, prm.size()) << "]; };\n";
-        src << "extern \"C\" __global__ void __launch_bounds__(" << T << ", " << (T >= 64 ? 2 : 1) << ") qse_pass("
+        // resident CTAs per SM the register budget allows at 128 registers per thread
+        const uint32_t min_blocks = std::max(1u, std::min(8u, 65536u / (T * 128u)));
+        src << "extern \"C\" __global__ void __launch_bounds__(" << T << ", " << min_blocks << ") qse_pass("
             << "double2* __restrict__ psi, double2* __restrict__ lam, const TermRec* __restrict__ terms, "
             << "const GroupRec* __restrict__ groups, double* __restrict__ slot_partial, const __grid_constant__ Prm P)\n{\n"
             << "  (void)lam; (void)terms; (void)groups; (void)slot_partial;\n"

@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <map>
+#include <set>
 #include <sstream>
 #include <tuple>
 
@@ -106,37 +107,145 @@ public:
         for (uint32_t b = 0; b < P.k; ++b) loc_[P.tile_phys[b]] = int(b);
     }
 
+    // Gates of the pass are emitted in a topological order of their
+    // dependency graph (b depends on an earlier a when they share a qubit on
+    // which either acts non-diagonally; SWAPs are already folded into the
+    // physical qubits).  Ready diagonal gates go first; then ready gates on
+    // the current register bits; only when none is left does the pass change
+    // register layout, to the bits with the most ready gates.  For the QFT
+    // this halves the layouts of program order (one per block of register bits).
     void run(const std::vector<Absorbed>& abs, double gphase)
     {
-        // tile-local bits needed in registers, in order
-        std::vector<int> need(abs.size(), -1);
-        for (size_t i = 0; i < abs.size(); ++i)
-            if (abs[i].cls == C_N1 || abs[i].cls == C_CX) need[i] = loc_[abs[i].pt];
-        need_ = &need;
-        choose_regs(0, nullptr);
+        const int m = int(abs.size());
+        std::vector<std::vector<int>> succ(m);
+        std::vector<int> indeg(m, 0);
+        {
+            std::vector<int> last_n(64, -1);
+            std::vector<std::vector<int>> dl(64);
+            auto edge = [&](int a, int b) {
+                succ[a].push_back(b);
+                ++indeg[b];
+            };
+            for (int i = 0; i < m; ++i) {
+                const Absorbed& a = abs[i];
+                if (a.cls == C_SWAP) continue;
+                uint64_t nq = 0, dq = 0;
+                if (a.cls == C_N1) nq = bit(a.pt);
+                else if (a.cls == C_CX) { nq = bit(a.pt); dq = bit(a.pc); }
+                else dq = a.psup;
+                for (uint64_t s = nq; s; s &= s - 1) {
+                    int q = __builtin_ctzll(s);
+                    if (last_n[q] >= 0) edge(last_n[q], i);
+                    for (int d : dl[q]) edge(d, i);
+                    last_n[q] = i;
+                    dl[q].clear();
+                }
+                for (uint64_t s = dq; s; s &= s - 1) {
+                    int q = __builtin_ctzll(s);
+                    if (last_n[q] >= 0) edge(last_n[q], i);
+                    dl[q].push_back(i);
+                }
+            }
+        }
+        std::set<int> ready_d, ready_n;
+        auto make_ready = [&](int i) {
+            if (abs[i].cls == C_DIAG) ready_d.insert(i);
+            else ready_n.insert(i);
+        };
+        int total = 0;
+        for (int i = 0; i < m; ++i) {
+            if (abs[i].cls == C_SWAP) continue;
+            ++total;
+            if (indeg[i] == 0) make_ready(i);
+        }
+        auto release = [&](int i) {
+            for (int s : succ[i])
+                if (--indeg[s] == 0) make_ready(s);
+        };
+        // register bits for a new layout: most ready gates, then most gates in the lookahead, then earliest
+        auto pick_regs = [&](const int* prev) {
+            std::vector<long long> score(P.k, 0);
+            std::vector<int> first(P.k, 1 << 30);
+            for (int i : ready_n) {
+                int b = loc_[abs[i].pt];
+                score[b] += 1000000;
+                first[b] = std::min(first[b], i);
+            }
+            int seen = 0;
+            for (int i = 0; i < m && seen < 64; ++i) {
+                if (abs[i].cls != C_N1 && abs[i].cls != C_CX) continue;
+                if (indeg[i] < 0) continue;  // already emitted
+                int b = loc_[abs[i].pt];
+                score[b] += 64 - seen;
+                first[b] = std::min(first[b], i);
+                ++seen;
+            }
+            std::vector<int> bits(P.k);
+            for (uint32_t b = 0; b < P.k; ++b) bits[b] = int(b);
+            std::stable_sort(bits.begin(), bits.end(), [&](int x, int y) {
+                if (score[x] != score[y]) return score[x] > score[y];
+                bool px = false, py = false;
+                if (prev)
+                    for (uint32_t r = 0; r < P.rb; ++r) { px |= prev[r] == x; py |= prev[r] == y; }
+                if (px != py) return px;
+                return first[x] < first[y];
+            });
+            std::vector<int> r(bits.begin(), bits.begin() + P.rb);
+            std::sort(r.begin(), r.end());
+            for (uint32_t i = 0; i < P.rb; ++i) reg_[i] = r[i];
+            nthr_ = 0;
+            for (uint32_t b = 0; b < P.k; ++b)
+                if (reg_pos(int(b)) < 0) thr_[nthr_++] = int(b);
+        };
+        pick_regs(nullptr);
         P.layout0 = add_layout(nullptr);
         scale_ = 1.0;
-        for (size_t i = 0; i < abs.size(); ++i) {
-            const Absorbed& a = abs[i];
+        P.order.clear();
+        P.phys_target.clear();
+        for (int i = 0; i < m; ++i)
+            if (abs[i].cls == C_SWAP) {
+                P.order.push_back(uint32_t(abs[i].src));
+                P.phys_target.push_back(0);
+                P.phys_control.push_back(0);
+                P.phys_support.push_back(0);
+            }
+        int emitted = 0;
+        while (emitted < total) {
+            int pick = -1;
+            if (!ready_d.empty()) {
+                pick = *ready_d.begin();
+                ready_d.erase(ready_d.begin());
+            } else {
+                for (int i : ready_n)
+                    if (reg_pos(loc_[abs[i].pt]) >= 0) { pick = i; break; }
+                if (pick < 0) {
+                    if (ready_n.empty()) fail(QSE_ERR_INVALID, "internal: pass schedule stalled");
+                    close_all(false, 1.0, 0.0);
+                    std::vector<int> prev(reg_, reg_ + P.rb);
+                    pick_regs(prev.data());
+                    KOp t{};
+                    t.kind = K_TRANSPOSE;
+                    t.g = uint16_t(add_layout(prev.data()));
+                    P.ops.push_back(t);
+                    continue;
+                }
+                ready_n.erase(pick);
+            }
+            indeg[pick] = -1;
+            ++emitted;
+            release(pick);
+            const Absorbed& a = abs[pick];
+            P.order.push_back(uint32_t(a.src));
+            P.phys_target.push_back(a.pt);
+            P.phys_control.push_back(a.pc);
+            P.phys_support.push_back(a.psup);
             const Gate& g = *a.g;
-            if (a.cls == C_SWAP) continue;
             if (a.cls == C_DIAG) {
                 if (opt_.grads && g.grad >= 0) emit_grad_diag(a);
                 add_diag_terms(a, gphase);
                 continue;
             }
-            int tb = loc_[a.pt];
-            int p = reg_pos(tb);
-            if (p < 0) {
-                close_all(false, 1.0, 0.0);
-                std::vector<int> prev(reg_, reg_ + P.rb);
-                choose_regs(i, &prev);
-                KOp t{};
-                t.kind = K_TRANSPOSE;
-                t.g = uint16_t(add_layout(prev.data()));
-                P.ops.push_back(t);
-                p = reg_pos(tb);
-            }
+            const int p = reg_pos(loc_[a.pt]);
             close_reg(p);
             if (opt_.grads && g.grad >= 0) emit_grad_pair(a, p);
             KOp op{};
@@ -173,7 +282,6 @@ private:
     int reg_[4] = {0, 0, 0, 0};
     int thr_[16];
     int nthr_ = 0;
-    const std::vector<int>* need_ = nullptr;
     double gphase_ = 0.0;
     double scale_ = 1.0;   // product of the 1/sqrt2 factors of the unscaled K_H applied so far
 
@@ -195,28 +303,6 @@ private:
         for (int i = 0; i < nthr_; ++i)
             if (thr_[i] == tb) return i;
         return -1;
-    }
-
-    // registers for the layout starting at gate index `from`: the next rb
-    // distinct needed bits, then bits of the previous layout, then high bits.
-    void choose_regs(size_t from, const std::vector<int>* prev)
-    {
-        std::vector<int> r;
-        auto has = [&](int b) { return std::find(r.begin(), r.end(), b) != r.end(); };
-        for (size_t i = from; i < need_->size() && r.size() < P.rb; ++i) {
-            int b = (*need_)[i];
-            if (b >= 0 && !has(b)) r.push_back(b);
-        }
-        if (prev)
-            for (int b : *prev)
-                if (r.size() < P.rb && !has(b)) r.push_back(b);
-        for (int b = int(P.k) - 1; b >= 0 && r.size() < P.rb; --b)
-            if (!has(b)) r.push_back(b);
-        std::sort(r.begin(), r.end());
-        for (uint32_t i = 0; i < P.rb; ++i) reg_[i] = r[i];
-        nthr_ = 0;
-        for (uint32_t b = 0; b < P.k; ++b)
-            if (reg_pos(int(b)) < 0) thr_[nthr_++] = int(b);
     }
 
     // Slot images for the shared-memory exchange from layout `prev` to the
@@ -470,7 +556,8 @@ Plan build(const std::vector<Gate>& gates, uint32_t n, const uint32_t* perm_in, 
                     if (nterms < opt.max_terms) {
                         uint64_t ps = 0;
                         for (uint64_t s = in.dset; s; s &= s - 1) ps |= bit(perm[__builtin_ctzll(s)]);
-                        abs.push_back(Absorbed{idx, &g, C_DIAG, perm[g.t], 0, ps});
+                        abs.push_back(Absorbed{idx, &g, C_DIAG, perm[g.t],
+                                               g.type == QSE_GATE_CPHASE ? perm[g.c] : 0u, ps});
                         ++nterms;
                         continue;
                     }
@@ -501,10 +588,6 @@ Plan build(const std::vector<Gate>& gates, uint32_t n, const uint32_t* perm_in, 
         uint64_t all = n >= 64 ? ~uint64_t(0) : (bit(n) - 1);
         prog.outer_mask = all & ~T;
         prog.ngates = uint32_t(abs.size());
-        for (const Absorbed& a : abs) {
-            prog.order.push_back(uint32_t(a.src));
-            prog.phys_target.push_back(a.pt);
-        }
         Lowering low(prog, n, opt);
         low.run(abs, gph);
         plan.passes.push_back(std::move(prog));
@@ -527,7 +610,8 @@ std::string describe(const Plan& p)
            << ",\"layouts\":" << pp.layouts.size() << ",\"gates\":" << pp.ngates
            << ",\"nondiag\":" << pp.n_nondiag << ",\"order\":[";
         for (size_t j = 0; j < pp.order.size(); ++j)
-            os << (j ? "," : "") << "[" << pp.order[j] << "," << pp.phys_target[j] << "]";
+            os << (j ? "," : "") << "[" << pp.order[j] << "," << pp.phys_target[j] << "," << pp.phys_control[j]
+               << "," << pp.phys_support[j] << "]";
         os << "],\"kinds\":[";
         for (size_t j = 0; j < pp.ops.size(); ++j) os << (j ? "," : "") << int(pp.ops[j].kind);
         os << "]}";

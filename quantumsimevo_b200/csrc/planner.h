@@ -87,7 +87,12 @@ struct PassProgram {
     std::vector<double> mats;       // 8 doubles per K_U matrix
     std::vector<int32_t> slot_src;  // gradient slot (local) -> gradient occurrence id
     std::vector<uint32_t> order;    // source-gate indices absorbed, in execution order
-    std::vector<uint32_t> phys_target;  // physical target of each absorbed gate (debug view)
+    // debug view, per entry of `order`: physical target, physical control
+    // (CNOT / CPHASE) and physical support (diagonal gates); SWAPs come first
+    // with zeros (they only relabel)
+    std::vector<uint32_t> phys_target;
+    std::vector<uint32_t> phys_control;
+    std::vector<uint64_t> phys_support;
     uint32_t ngates = 0;            // source gates absorbed
     uint32_t n_nondiag = 0;
 };

@@ -1,0 +1,113 @@
+"""The reference's own Circuit / StateVector / Noise (compiled from its sources
+into oracle/_ref) running on this project's drop-in backend
+CircuitUnitaryOperationB200, against the same reference code on its scalar
+backend; plus the torch.autograd binding."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+import oracle_ffi as O
+from quantumsimevo_b200 import _lib as L
+from quantumsimevo_b200 import workloads as W
+from quantumsimevo_b200.autograd import ParametrizedCircuit, QuantumLayer
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ref():
+    r = O.load_reference(gpu=True)
+    if r is None:
+        pytest.skip("oracle/_ref/libqse_ref_gpu.so not built")
+    r.ref_set_quiet(1)
+    return r
+
+
+@pytest.mark.parametrize("n", [1, 3, 6, 10, 14])
+def test_reference_circuit_on_b200_adapter(ref, n):
+    for rep in range(2):
+        ops = W.random_circuit(n, 30 * n + 10, 8000 + 11 * n + rep, with_2x2=False)
+        want = O.ref_run(ref, n, ops, backend=0)     # reference Circuit, scalar backend
+        got = O.ref_run(ref, n, ops, backend=3)      # reference Circuit, CircuitUnitaryOperationB200
+        assert np.max(np.abs(got - want)) <= 1e-12
+
+
+def test_reference_gpu_backend_rebuilt_for_sm100(ref):
+    # the reference's own CUDA backend compiled for sm_100a (the plain-kernel baseline)
+    n = 12
+    ops = W.random_circuit(n, 300, 81, with_2x2=False)
+    want = O.ref_run(ref, n, ops, backend=0)
+    got = O.ref_run(ref, n, ops, backend=2)
+    assert np.max(np.abs(got - want)) <= 1e-12
+
+
+def test_reference_noise_through_adapter(ref):
+    # Circuit(N, true): Noise(N, 42, 1) draws from mt19937 and applies X/Z through the backend
+    n = 9
+    ops = W.random_circuit(n, 400, 82, with_2x2=False)
+    outs = []
+    for backend in (0, 3):
+        assert ref.ref_set_backend(backend) == 0
+        h = ref.ref_circuit_new(n, 1)
+        a = np.ascontiguousarray(ops)
+        ref.ref_circuit_add_many(h, a.ctypes.data_as(C.c_void_p), len(a))
+        ref.ref_circuit_execute(h, 0)
+        ref.ref_circuit_execute(h, 0)   # the queue is replayed and the noise re-applied
+        st = np.empty(1 << n, dtype=np.complex128)
+        ref.ref_circuit_state(h, st.ctypes.data_as(C.c_void_p))
+        ref.ref_circuit_free(h)
+        outs.append(st)
+    ref.ref_set_backend(0)
+    assert np.max(np.abs(outs[0] - outs[1])) <= 1e-12
+
+
+def test_adapter_flush_and_host_dirty(ref):
+    # per-gate through the backend object: markHostDirty re-uploads host edits
+    n = 8
+    be = ref.ref_backend_new(3)
+    sv = ref.ref_statevector_new(n)
+    ops = W.random_circuit(n, 60, 83, with_2x2=True)
+    a = np.ascontiguousarray(ops)
+    assert ref.ref_backend_apply(be, sv, a.ctypes.data_as(C.c_void_p), len(a)) == 0
+    ref.ref_backend_flush(be)
+    st = np.empty(1 << n, dtype=np.complex128)
+    ref.ref_statevector_get(sv, st.ctypes.data_as(C.c_void_p))
+    assert np.max(np.abs(st - O.run(n, ops))) <= 1e-12
+    # edit on the host, mark dirty, apply more gates
+    edited = np.roll(st, 3)
+    ref.ref_statevector_set(sv, edited.ctypes.data_as(C.c_void_p))
+    ref.ref_backend_mark_host_dirty(be)
+    more = np.ascontiguousarray(W.random_circuit(n, 20, 84, with_2x2=True))
+    assert ref.ref_backend_apply(be, sv, more.ctypes.data_as(C.c_void_p), len(more)) == 0
+    ref.ref_backend_flush(be)
+    ref.ref_statevector_get(sv, st.ctypes.data_as(C.c_void_p))
+    assert np.max(np.abs(st - O.run_on(edited, n, more))) <= 1e-12
+    ref.ref_statevector_free(sv)
+    ref.ref_backend_free(be)
+
+
+def test_torch_autograd_matches_oracle_and_fd():
+    n = 10
+    ops, params, edges, obs_t = W.qaoa_maxcut(n, 2, seed=90)
+    pc = ParametrizedCircuit(n, ops, *obs_t)
+    layer = QuantumLayer(pc, params)
+    val = layer()
+    val.backward()
+    obs, keep = L.observable(*obs_t)
+    vw, gw = O.adjoint(n, ops, params, obs)
+    assert abs(val.item() - vw) <= 1e-10
+    assert np.max(np.abs(layer.params.grad.numpy() - gw)) <= 1e-10
+    # central finite differences, h = 1e-6: round-off limits agreement to ~1e-7
+    h = 1e-6
+    for k in range(len(params)):
+        pp, pm = params.copy(), params.copy()
+        pp[k] += h
+        pm[k] -= h
+        fd = (pc.value(pp) - pc.value(pm)) / (2 * h)
+        assert abs(fd - gw[k]) <= 1e-7 * max(1.0, abs(gw[k]))
+    # no-grad forward
+    with torch.no_grad():
+        v2 = pc.expectation(torch.tensor(params))
+    assert abs(v2.item() - vw) <= 1e-10
