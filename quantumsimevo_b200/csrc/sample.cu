@@ -37,6 +37,10 @@ constexpr int kBT = 256;            // threads per block
 constexpr int kEPT = 16;            // elements per thread
 constexpr int kBS = kBT * kEPT;     // elements per block (4096)
 constexpr uint64_t kTwo53 = uint64_t(1) << 53;
+constexpr int kPad = kEPT + 1;      // staging-buffer row stride (doubles)
+
+// staging-buffer position of block element i (row i / kEPT, column i % kEPT)
+__device__ __forceinline__ uint32_t stage_slot(uint32_t i) { return (i / kEPT) * kPad + (i % kEPT); }
 
 // Block folds on the grids of two adjacent binades, e and e+1: the running sum
 // at the block is known only approximately, and near a binade boundary (for a
@@ -156,7 +160,8 @@ __device__ void block_scan_maps(uint64_t t0, uint64_t t1, uint64_t& ex0, uint64_
 // as p[0..kEPT) per thread (element index = tid*kEPT + j), starting from the
 // exact running sum c_in.  Writes the values to out (if non-null) and returns
 // the block's final sum.  Must be called by all threads of the block.
-__device__ double block_exact(const double (&p)[kEPT], uint32_t cnt, double c_in, double* out, uint64_t* sh)
+__device__ double block_exact(const double (&p)[kEPT], uint32_t cnt, double c_in, double* out, uint64_t* sh,
+                              double* stage)
 {
     __shared__ double s_c;
     __shared__ int s_t;
@@ -211,7 +216,7 @@ __device__ double block_exact(const double (&p)[kEPT], uint32_t cnt, double c_in
 #pragma unroll
         for (int j = 0; j < kEPT; ++j) {
             uint32_t i = tid * kEPT + j;
-            if (i >= pos && i < t && out) out[i] = double(Ci[j]) * G;
+            if (i >= pos && i < t && out) stage[tid * kPad + j] = double(Ci[j]) * G;
             if (t < cnt && i >= pos && i + 1 == t) s_c = double(Ci[j]) * G;   // c_{t-1}
             if (t == cnt && i + 1 == cnt) s_c = double(Ci[j]) * G;
         }
@@ -226,7 +231,7 @@ __device__ double block_exact(const double (&p)[kEPT], uint32_t cnt, double c_in
             for (int j = 0; j < kEPT; ++j)
                 if (j == int(t % kEPT)) pt = p[j];
             double ct = __dadd_rn(prev, pt);
-            if (out) out[t] = ct;
+            if (out) stage[stage_slot(t)] = ct;
             s_c = ct;
         }
         __syncthreads();
@@ -234,37 +239,136 @@ __device__ double block_exact(const double (&p)[kEPT], uint32_t cnt, double c_in
         pos = t + 1;
         __syncthreads();
     }
+    if (out) {
+        // coalesced copy of the staged cumulative values
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kEPT; ++j) {
+            const uint32_t i = j * kBT + tid;
+            if (i < cnt) out[i] = stage[stage_slot(i)];
+        }
+    }
     return c;
 }
 
-__device__ __forceinline__ void load_block_p(const double2* __restrict__ amp, uint64_t base, uint32_t cnt,
-                                             const PermMap& pm, double (&p)[kEPT])
+// Probabilities of block elements [base, base + kBS) of the logical-order
+// probability array: element i belongs to thread i / kEPT, slot i % kEPT.  The
+// array is read coalesced into the padded staging buffer and each thread then
+// picks up its kEPT consecutive values (row stride kPad keeps the 8-byte
+// reads free of bank conflicts).
+__device__ __forceinline__ void load_block_prob(const double* prob, uint64_t base, double (&p)[kEPT], double* stage)
 {
+    __syncthreads();  // earlier readers of the staging buffer are done
 #pragma unroll
     for (int j = 0; j < kEPT; ++j) {
-        uint32_t i = threadIdx.x * kEPT + j;
-        p[j] = i < cnt ? norm2(amp[phys_index(base + i, pm)]) : 0.0;
+        const uint32_t i = j * kBT + threadIdx.x;
+        stage[stage_slot(i)] = prob[base + i];
     }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kEPT; ++j) p[j] = stage[threadIdx.x * kPad + j];
 }
 
-__global__ void __launch_bounds__(kBT) k_cdf_bsum(const double2* __restrict__ amp, uint64_t size, PermMap pm,
-                                                  double* __restrict__ bsum)
+__device__ __forceinline__ void block_sum_store(double s, double* out)
 {
     __shared__ double sh[kBT / 32];
-    double p[kEPT];
-    uint64_t base = uint64_t(blockIdx.x) * kBS;
-    load_block_p(amp, base, kBS, pm, p);
-    double s = 0.0;
-#pragma unroll
-    for (int j = 0; j < kEPT; ++j) s += p[j];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
     __syncthreads();
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int w = 0; w < kBT / 32; ++w) t += sh[w];
-        bsum[blockIdx.x] = t;
+        *out = t;
     }
+}
+
+// Identity qubit map: prob[i] = |amp[i]|^2 (coalesced), block sums on the way.
+__global__ void __launch_bounds__(kBT) k_prob_identity(const double2* __restrict__ amp, double* __restrict__ prob,
+                                                       double* __restrict__ bsum)
+{
+    const uint64_t base = uint64_t(blockIdx.x) * kBS;
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < kEPT; ++j) {
+        const uint64_t i = base + j * kBT + threadIdx.x;
+        const double v = norm2(amp[i]);
+        prob[i] = v;
+        s += v;
+    }
+    block_sum_store(s, bsum + blockIdx.x);
+}
+
+// Relabelled qubits (after SWAPs): the logical-order probability array is a
+// bit permutation of the physical amplitudes.  Each CTA takes the 4096
+// amplitudes spanned by 12 physical bits S that contain physical bits 0..4
+// (contiguous 512-byte reads) and the physical images of logical bits 0..6
+// (contiguous 1 KiB writes of probabilities), and transposes through shared
+// memory.
+struct GatherPlan {
+    uint64_t outer_mask;      // physical bits outside S
+    uint8_t sphys[12];        // S ascending (tile order for the reads)
+    uint8_t slog[12];         // logical images of S, ascending (tile order for the writes)
+    uint8_t wsrc[12];         // write-order bit b' -> read-order bit
+    uint8_t pad[4];
+    uint8_t inv[64];          // physical bit -> logical bit
+};
+
+__global__ void __launch_bounds__(kBT) k_prob_gather(const double2* __restrict__ amp, double* __restrict__ prob,
+                                                     GatherPlan g)
+{
+    __shared__ double sm[kBS];
+    const uint32_t t = threadIdx.x;
+    uint64_t ob = 0, lb = 0;
+    {
+        uint64_t c = blockIdx.x, m = g.outer_mask;
+        while (m) {
+            const uint32_t b = __ffsll((long long)m) - 1;
+            m &= m - 1;
+            if (c & 1) {
+                ob |= uint64_t(1) << b;
+                lb |= uint64_t(1) << g.inv[b];
+            }
+            c >>= 1;
+        }
+    }
+    uint64_t tr = ob, tw = lb;
+    uint32_t ts = 0;
+    for (int b = 0; b < 8; ++b)
+        if ((t >> b) & 1) {
+            tr |= uint64_t(1) << g.sphys[b];
+            tw |= uint64_t(1) << g.slog[b];
+            ts |= 1u << g.wsrc[b];
+        }
+#pragma unroll
+    for (int j = 0; j < kEPT; ++j) {
+        uint64_t off = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+            if ((j >> b) & 1) off |= uint64_t(1) << g.sphys[8 + b];
+        sm[j * kBT + t] = norm2(amp[tr | off]);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kEPT; ++j) {
+        uint64_t off = 0;
+        uint32_t so = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+            if ((j >> b) & 1) {
+                off |= uint64_t(1) << g.slog[8 + b];
+                so |= 1u << g.wsrc[8 + b];
+            }
+        prob[tw | off] = sm[ts | so];
+    }
+}
+
+__global__ void __launch_bounds__(kBT) k_prob_bsum(const double* __restrict__ prob, double* __restrict__ bsum)
+{
+    const uint64_t base = uint64_t(blockIdx.x) * kBS;
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < kEPT; ++j) s += prob[base + j * kBT + threadIdx.x];
+    block_sum_store(s, bsum + blockIdx.x);
 }
 
 // single CTA: approximate exclusive prefix -> grid guess per block
@@ -298,7 +402,7 @@ __global__ void __launch_bounds__(1024) k_cdf_guess(const double* __restrict__ b
     }
 }
 
-__global__ void __launch_bounds__(kBT) k_cdf_summ(const double2* __restrict__ amp, PermMap pm,
+__global__ void __launch_bounds__(kBT) k_cdf_summ(const double* __restrict__ prob,
                                                   const int32_t* __restrict__ guess, Summ* __restrict__ summ)
 {
     __shared__ uint64_t sh[160];
@@ -307,8 +411,9 @@ __global__ void __launch_bounds__(kBT) k_cdf_summ(const double2* __restrict__ am
         if (threadIdx.x == 0) summ[blockIdx.x] = Summ{{{0, 0}, {0, 0}}, e, 0};
         return;
     }
+    __shared__ double stage[kBT * kPad];
     double p[kEPT];
-    load_block_p(amp, uint64_t(blockIdx.x) * kBS, kBS, pm, p);
+    load_block_prob(prob, uint64_t(blockIdx.x) * kBS, p, stage);
     Summ out{{{0, 0}, {0, 0}}, e, 0};
     for (int k = 0; k < 2; ++k) {
         uint64_t t0 = 0, t1 = 0;
@@ -335,11 +440,12 @@ __global__ void __launch_bounds__(kBT) k_cdf_summ(const double2* __restrict__ am
 
 // single CTA: exact running sum block by block; blocks whose guess does not
 // hold are folded exactly here.  cin[b] = exact sum before block b; cin[nb] = total.
-__global__ void __launch_bounds__(kBT) k_cdf_chain(const double2* __restrict__ amp, PermMap pm,
+__global__ void __launch_bounds__(kBT) k_cdf_chain(const double* __restrict__ prob,
                                                    const Summ* __restrict__ summ, uint32_t nb, double* __restrict__ cin,
                                                    uint32_t* __restrict__ stats)
 {
     __shared__ uint64_t sh[160];
+    __shared__ double stage[kBT * kPad];
     uint32_t n_fast = 0, n_slow = 0, n_exact = 0;  // chunk / block statistics (thread 0)
     __shared__ double s_c;
     __shared__ int s_slow;
@@ -406,8 +512,8 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double2* __restrict__ a
             if (s_slow) {
                 ++n_exact;
                 double p[kEPT];
-                load_block_p(amp, uint64_t(b) * kBS, kBS, pm, p);
-                double cc = block_exact(p, kBS, s_c, nullptr, sh);
+                load_block_prob(prob, uint64_t(b) * kBS, p, stage);
+                double cc = block_exact(p, kBS, s_c, nullptr, sh, stage);
                 if (t == 0) s_c = cc;
             }
             __syncthreads();
@@ -424,13 +530,14 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double2* __restrict__ a
     }
 }
 
-__global__ void __launch_bounds__(kBT) k_cdf_write(const double2* __restrict__ amp, PermMap pm,
-                                                   const double* __restrict__ cin, double* __restrict__ cdf)
+// in place: the probabilities of each block are replaced by their exact cumulative sums
+__global__ void __launch_bounds__(kBT) k_cdf_write(const double* __restrict__ cin, double* __restrict__ cdf)
 {
     __shared__ uint64_t sh[160];
+    __shared__ double stage[kBT * kPad];
     double p[kEPT];
-    load_block_p(amp, uint64_t(blockIdx.x) * kBS, kBS, pm, p);
-    block_exact(p, kBS, cin[blockIdx.x], cdf + uint64_t(blockIdx.x) * kBS, sh);
+    load_block_prob(cdf, uint64_t(blockIdx.x) * kBS, p, stage);
+    block_exact(p, kBS, cin[blockIdx.x], cdf + uint64_t(blockIdx.x) * kBS, sh, stage);
 }
 
 // small states (< one block): the sequential chain itself
@@ -509,6 +616,33 @@ struct CdfView {
     uint32_t bs;
 };
 
+// Tile of the gather: physical bits 0..4 and the physical images of logical
+// bits 0..6, padded with the lowest remaining physical bits to 12 (n >= 12).
+GatherPlan make_gather(const qse_state* st)
+{
+    GatherPlan g{};
+    uint64_t S = 0x1Full;
+    for (uint32_t q = 0; q < 7; ++q) S |= uint64_t(1) << st->perm[q];
+    for (uint32_t q = 0; q < st->n && __builtin_popcountll(S) < 12; ++q) S |= uint64_t(1) << q;
+    for (uint32_t q = 0; q < st->n; ++q) g.inv[st->perm[q]] = uint8_t(q);
+    int b = 0;
+    for (uint32_t q = 0; q < st->n; ++q)
+        if ((S >> q) & 1) g.sphys[b++] = uint8_t(q);
+    uint64_t Slog = 0;
+    for (int i = 0; i < 12; ++i) Slog |= uint64_t(1) << g.inv[g.sphys[i]];
+    b = 0;
+    for (uint32_t q = 0; q < st->n; ++q)
+        if ((Slog >> q) & 1) g.slog[b++] = uint8_t(q);
+    for (int i = 0; i < 12; ++i) {
+        const uint32_t phys = st->perm[g.slog[i]];
+        for (int r = 0; r < 12; ++r)
+            if (g.sphys[r] == phys) g.wsrc[i] = uint8_t(r);
+    }
+    const uint64_t all = st->n >= 64 ? ~uint64_t(0) : ((uint64_t(1) << st->n) - 1);
+    g.outer_mask = all & ~S;
+    return g;
+}
+
 // Exact cumulative array of the current amplitudes, cached per state until
 // the amplitudes change (sample() followed by measure() builds it once).
 CdfView build_cdf(qse_state* st)
@@ -544,14 +678,22 @@ CdfView build_cdf(qse_state* st)
         Summ* summ = reinterpret_cast<Summ*>(base + off_summ);
         v.nb = nb;
         v.bs = kBS;
-        k_cdf_bsum<<<nb, kBT, 0, ctx->stream>>>(amp, size, pm, bsum);
+        // probabilities in logical order into the cumulative array (transformed in place below)
+        if (pm.identity) {
+            k_prob_identity<<<nb, kBT, 0, ctx->stream>>>(amp, v.cdf, bsum);
+            count_launch(ctx);
+        } else {
+            GatherPlan g = make_gather(st);
+            k_prob_gather<<<unsigned(size / kBS), kBT, 0, ctx->stream>>>(amp, v.cdf, g);
+            k_prob_bsum<<<nb, kBT, 0, ctx->stream>>>(v.cdf, bsum);
+            count_launch(ctx, 2);
+        }
         k_cdf_guess<<<1, 1024, 0, ctx->stream>>>(bsum, nb, guess);
-        k_cdf_summ<<<nb, kBT, 0, ctx->stream>>>(amp, pm, guess, summ);
-        k_cdf_chain<<<1, kBT, 0, ctx->stream>>>(amp, pm, summ, nb, v.cin,
-                                                reinterpret_cast<uint32_t*>(v.cin + nb + 1));
-        k_cdf_write<<<nb, kBT, 0, ctx->stream>>>(amp, pm, v.cin, v.cdf);
+        k_cdf_summ<<<nb, kBT, 0, ctx->stream>>>(v.cdf, guess, summ);
+        k_cdf_chain<<<1, kBT, 0, ctx->stream>>>(v.cdf, summ, nb, v.cin, reinterpret_cast<uint32_t*>(v.cin + nb + 1));
+        k_cdf_write<<<nb, kBT, 0, ctx->stream>>>(v.cin, v.cdf);
         QSE_CUDA(cudaGetLastError());
-        count_launch(ctx, 5);
+        count_launch(ctx, 4);
     }
     st->cdf_values = v.cdf;
     st->cdf_block_start = v.cin;
