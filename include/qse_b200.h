@@ -280,9 +280,42 @@ QSE_API int qse_batch_run(qse_batch* b, const double* params, double* values, do
 /* device-resident variant: d_params / d_values / d_grads are device pointers; no host copies, no sync */
 QSE_API int qse_batch_run_device(qse_batch* b, const double* d_params, double* d_values, double* d_grads);
 QSE_API int qse_batch_total_params(const qse_batch* b, size_t* n);
-/* choose tile shape per width bucket by timing candidates; cache_path (may be NULL) holds JSON */
+/* Times candidate configurations on this batch (block shape / tile qubits, gates
+ * fused per pass, how many tiles a circuit may have and still run start to end
+ * in one CTA) with the parameters of the last run (zeros before the first) and
+ * keeps the fastest.  cache_path (may be NULL): a JSON file of earlier results,
+ * keyed by the batch's structure and the device; read first, updated after. */
 QSE_API int qse_batch_autotune(qse_batch* b, const char* cache_path);
+/* 1 (default): every run replays one CUDA graph [reset counters, bind angles,
+ * persistent kernel, reductions]; 0: the same launches issued one by one. */
 QSE_API int qse_batch_use_graph(qse_batch* b, int enabled);
+
+typedef struct qse_batch_config {
+    uint32_t threads;       /* CTA size, a power of two in 32..512                       */
+    uint32_t reg_bits;      /* 2^reg_bits amplitudes per thread: 2 or 3                   */
+                            /* tile qubits k = log2(threads) + reg_bits                   */
+    uint32_t max_gates;     /* non-diagonal gates per pass, 0 = no cap                    */
+    uint32_t chain_tiles;   /* circuits with at most this many tiles per pass run as one
+                               work item (one CTA, start to end); >= 1                    */
+    uint32_t ctas_per_sm;   /* persistent CTAs per SM, 0 = as many as fit                 */
+} qse_batch_config;
+QSE_API int qse_batch_set_config(qse_batch* b, const qse_batch_config* cfg);
+QSE_API int qse_batch_get_config(const qse_batch* b, qse_batch_config* cfg);
+
+typedef struct qse_batch_stats {
+    uint64_t passes;        /* planned passes, forward + reverse, all circuits            */
+    uint64_t items;         /* work-queue entries of one run                              */
+    uint64_t tile_visits;   /* (pass, tile) pairs processed per run                       */
+    uint64_t hbm_bytes;     /* algorithmic HBM bytes of one run: 32 B per amplitude per
+                               forward pass and 64 B per reverse pass of circuits that
+                               span several tiles (single-tile circuits stay on chip)     */
+    uint64_t occurrences;   /* parameterised gate occurrences (gradient slots)            */
+    uint32_t grid;          /* persistent CTAs                                            */
+    uint32_t smem_bytes;    /* dynamic shared memory per CTA                              */
+    double   last_ms;       /* device time of the last run (0 if none)                    */
+    double   plan_ms;       /* host time of the last planning                             */
+} qse_batch_stats;
+QSE_API int qse_batch_get_stats(qse_batch* b, qse_batch_stats* out);
 
 #ifdef __cplusplus
 }

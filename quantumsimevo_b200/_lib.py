@@ -54,6 +54,17 @@ class QseBatchCircuit(C.Structure):
                 ("obs", QseObservable)]
 
 
+class QseBatchConfig(C.Structure):
+    _fields_ = [("threads", C.c_uint32), ("reg_bits", C.c_uint32), ("max_gates", C.c_uint32),
+                ("chain_tiles", C.c_uint32), ("ctas_per_sm", C.c_uint32)]
+
+
+class QseBatchStats(C.Structure):
+    _fields_ = [("passes", C.c_uint64), ("items", C.c_uint64), ("tile_visits", C.c_uint64),
+                ("hbm_bytes", C.c_uint64), ("occurrences", C.c_uint64), ("grid", C.c_uint32),
+                ("smem_bytes", C.c_uint32), ("last_ms", C.c_double), ("plan_ms", C.c_double)]
+
+
 assert C.sizeof(QseOp) == 104
 
 
@@ -130,6 +141,9 @@ _SIGS = {
     "qse_batch_total_params": ([_vp, C.POINTER(_sz)], C.c_int),
     "qse_batch_autotune": ([_vp, C.c_char_p], C.c_int),
     "qse_batch_use_graph": ([_vp, C.c_int], C.c_int),
+    "qse_batch_set_config": ([_vp, C.POINTER(QseBatchConfig)], C.c_int),
+    "qse_batch_get_config": ([_vp, C.POINTER(QseBatchConfig)], C.c_int),
+    "qse_batch_get_stats": ([_vp, C.POINTER(QseBatchStats)], C.c_int),
 }
 
 for _name, (_args, _res) in _SIGS.items():

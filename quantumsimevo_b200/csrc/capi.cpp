@@ -19,6 +19,8 @@ namespace {
 thread_local std::string g_last_error;
 }
 
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
 [[noreturn]] void fail(int status, const std::string& msg) { throw Error(status, msg); }
 
 void cuda_check(cudaError_t e, const char* what, const char* file, int line)

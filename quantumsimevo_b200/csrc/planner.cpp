@@ -258,8 +258,12 @@ public:
                 case QSE_GATE_H: op.kind = K_H; scale_ *= kInvSqrt2; break;
                 case QSE_GATE_X: op.kind = K_X; break;
                 case QSE_GATE_Y: op.kind = K_Y; break;
-                case QSE_GATE_RX: op.kind = K_RX; op.a = std::cos(g.theta / 2.0); op.b = std::sin(g.theta / 2.0); break;
-                case QSE_GATE_RY: op.kind = K_RY; op.a = std::cos(g.theta / 2.0); op.b = std::sin(g.theta / 2.0); break;
+                case QSE_GATE_RX: case QSE_GATE_RY:
+                    op.kind = g.type == QSE_GATE_RX ? K_RX : K_RY;
+                    op.a = std::cos(g.theta / 2.0);
+                    op.b = std::sin(g.theta / 2.0);
+                    P.op_angles.push_back(AngleRef{uint32_t(P.ops.size()), uint32_t(a.src)});
+                    break;
                 case QSE_GATE_2X2:
                     op.kind = K_U;
                     op.g = uint16_t(P.mats.size() / 8);
@@ -271,7 +275,8 @@ public:
             P.ops.push_back(op);
             P.n_nondiag++;
         }
-        close_all(true, scale_ * std::cos(gphase_), scale_ * std::sin(gphase_));
+        if (opt_.keep_gphase) close_all(true, scale_ * std::cos(gphase_), scale_ * std::sin(gphase_));
+        else close_all(true, scale_, 0.0);
     }
 
 private:
@@ -289,6 +294,7 @@ private:
         uint8_t kind, p, f;
         uint16_t tcond;
         std::vector<TermRec> terms;
+        std::vector<int32_t> src;   // source gate of each term (-1: constant angle)
     };
     std::map<std::tuple<int, int, int>, OG> open_;
 
@@ -380,7 +386,7 @@ private:
         }
     }
 
-    void add_term(uint64_t sup, double theta)
+    void add_term(uint64_t sup, double theta, int32_t src)
     {
         if (sup == 0) { gphase_ += theta; return; }
         uint8_t f;
@@ -393,20 +399,21 @@ private:
         auto key = std::make_tuple(kind, key2, int(tc));
         auto it = open_.find(key);
         if (it == open_.end()) {
-            OG og{uint8_t(kind), uint8_t(kind == K_ACC_REG ? __builtin_ctz(f) : 0), f, tc, {}};
+            OG og{uint8_t(kind), uint8_t(kind == K_ACC_REG ? __builtin_ctz(f) : 0), f, tc, {}, {}};
             it = open_.emplace(key, std::move(og)).first;
         }
         it->second.terms.push_back(TermRec{oc, theta});
+        it->second.src.push_back(src);
     }
 
     void add_diag_terms(const Absorbed& a, double& /*unused*/)
     {
         const Gate& g = *a.g;
         switch (g.type) {
-        case QSE_GATE_Z: add_term(a.psup, M_PI); break;
-        case QSE_GATE_PHASE: case QSE_GATE_CPHASE: case QSE_GATE_MCPHASE: add_term(a.psup, g.theta); break;
+        case QSE_GATE_Z: add_term(a.psup, M_PI, -1); break;
+        case QSE_GATE_PHASE: case QSE_GATE_CPHASE: case QSE_GATE_MCPHASE: add_term(a.psup, g.theta, int32_t(a.src)); break;
         case QSE_GATE_RZ:  // diag(e^{-it/2}, e^{it/2}) = e^{-it/2} diag(1, e^{it})
-            add_term(a.psup, g.theta);
+            add_term(a.psup, g.theta, int32_t(a.src));
             gphase_ += -g.theta / 2.0;
             break;
         default: fail(QSE_ERR_UNSUPPORTED, "internal: unexpected diagonal type");
@@ -419,6 +426,8 @@ private:
         gr.first = uint32_t(P.terms.size());
         gr.count = uint32_t(og.terms.size());
         gr.direct = og.kind == K_PHD ? 1u : 0u;
+        for (size_t i = 0; i < og.src.size(); ++i)
+            if (og.src[i] >= 0) P.term_angles.push_back(AngleRef{uint32_t(P.terms.size() + i), uint32_t(og.src[i])});
         P.terms.insert(P.terms.end(), og.terms.begin(), og.terms.end());
         P.groups.push_back(gr);
         return uint16_t(P.groups.size() - 1);

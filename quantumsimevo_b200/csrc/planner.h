@@ -74,6 +74,14 @@ struct GroupRec {      // terms [first, first+count) summed per CTA; direct grou
     uint32_t pad;
 };
 
+// An angle-carrying record of a pass and the source gate it came from: a
+// K_RX / K_RY op (a, b) = (cos, sin)(theta/2), or a diagonal term's theta.
+// Lets a caller rebind angles on the device without planning again.
+struct AngleRef {
+    uint32_t index;   // into PassProgram::ops or PassProgram::terms
+    uint32_t src;     // source-gate index in the planner input
+};
+
 struct PassProgram {
     uint32_t k = 0;                 // tile qubits
     uint32_t rb = 4;                // register bits per thread
@@ -86,6 +94,8 @@ struct PassProgram {
     std::vector<GroupRec> groups;
     std::vector<double> mats;       // 8 doubles per K_U matrix
     std::vector<int32_t> slot_src;  // gradient slot (local) -> gradient occurrence id
+    std::vector<AngleRef> op_angles;    // K_RX / K_RY ops
+    std::vector<AngleRef> term_angles;  // terms of PHASE / RZ / CPHASE / MCPHASE gates
     std::vector<uint32_t> order;    // source-gate indices absorbed, in execution order
     // debug view, per entry of `order`: physical target, physical control
     // (CNOT / CPHASE) and physical support (diagonal gates); SWAPs come first
@@ -114,6 +124,9 @@ struct Options {
     uint32_t max_gates = 0;      // 0 = no cap on non-diagonal gates per pass
     uint32_t max_terms = 1024;   // diagonal terms per pass (shared-memory group table)
     bool grads = false;          // emit K_GRAD_* for gates with grad >= 0
+    bool keep_gphase = true;     // false: drop RZ's global phase (expectations and gradients
+                                 // do not see it; the pass programs then depend on angles
+                                 // only through op_angles / term_angles)
 };
 
 struct Plan {

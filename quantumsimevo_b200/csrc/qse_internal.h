@@ -22,6 +22,7 @@ struct Error : std::runtime_error {
 };
 
 [[noreturn]] void fail(int status, const std::string& msg);
+void set_last_error(const std::string& msg);   // qse_last_error() text of the calling thread
 void cuda_check(cudaError_t e, const char* what, const char* file, int line);
 #define QSE_CUDA(call) ::qse::cuda_check((call), #call, __FILE__, __LINE__)
 

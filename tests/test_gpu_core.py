@@ -52,6 +52,25 @@ def test_fused_random_circuits(dev, n, k):
         assert err <= TOL, (rep, err, stats.passes)
 
 
+@pytest.mark.parametrize("n,k", [(6, 5), (12, 12), (14, 10)])
+def test_interpreter_kernel_without_jit(dev, n, k):
+    """The generic pass kernel (interpreter of the planned programs) that runs
+    when the NVRTC-specialised kernels are switched off; forward and adjoint."""
+    L.check(L.lib.qse_ctx_set_jit(dev.handle, 0))
+    try:
+        ops = W.random_circuit(n, 25 * n, 5000 + n)
+        got, _ = run_gpu(dev, n, ops, fusion=True, k=k)
+        assert np.max(np.abs(got - O.run(n, ops))) <= TOL
+        qops, params, _, obs_t = W.qaoa_maxcut(n, 2, seed=50 + n)
+        v, g = _adjoint(dev, n, qops, params, obs_t)
+        obs, keep = L.observable(*obs_t)
+        vw, gw = O.adjoint(n, qops, params, obs)
+        assert abs(v - vw) <= 1e-10
+        assert np.max(np.abs(g - gw)) <= 1e-10
+    finally:
+        L.check(L.lib.qse_ctx_set_jit(dev.handle, 1))
+
+
 def test_fused_gate_cap_and_tiles(dev):
     n = 15
     ops = W.random_circuit(n, 400, 42)
