@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--qubits", type=int, default=N_QUBITS)
     ap.add_argument("--shots", type=int, default=SHOTS)
     ap.add_argument("--no-qaoa", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-gates", type=int, default=0, help="gates in the CPU sample (0 = auto)")
     ap.add_argument("--tile", type=int, default=0, help="tile qubits of the fused passes (0 = library default)")
@@ -347,6 +348,9 @@ def main():
     qaoa = None
     if rank == 0 and not args.no_qaoa:
         qaoa = bench_qaoa(dev, L, W, np)
+    batch = None
+    if rank == 0 and not args.no_batch:
+        batch = bench_batch(dev, L, W, np, steps=args.steps, warmup=args.warmup)
 
     barrier()
     if rank == 0:
@@ -372,6 +376,7 @@ def main():
             "clocks": clk,
             "cpu_baseline": cpu,
             "qaoa": qaoa,
+            "batch": batch,
         }
         print(json.dumps(line))
     if dist:
@@ -449,6 +454,124 @@ def bench_qaoa(dev, L, W, np):
         "plain_execute_ms": t_plain * 1e3,
         "param_shift_evals_per_grad": evals,
         "timing": "host wall clock around synchronous C-ABI calls; plain param-shift extrapolated from 3 executes",
+    }
+
+
+def bench_batch(dev, L, W, np, steps=5, warmup=3, autotune=True, count=512):
+    """512 hardware-efficient-ansatz circuits (width U{10..22}, depth U{4..12}
+    layers of RY+RZ per qubit and a CNOT ring, observable sum_i Z_i): forward
+    <O> and the full adjoint gradient of every circuit per run, one persistent
+    kernel replayed as a CUDA graph.  Baseline: the parameter-shift rule with
+    one kernel per gate (2 executes per parameterised occurrence), timed on a
+    width-stratified sample of the same circuits and summed over the batch."""
+    import torch
+
+    from quantumsimevo_b200.batch import Batch
+    from quantumsimevo_b200.circuit import StateVector
+    hb = W.hea_batch(count, 10, 22, 4, 12, seed=5)
+    circs = [(w, ops, len(p), obs) for (w, ops, p, obs) in hb]
+    params = np.concatenate([p for (_, _, p, _) in hb])
+    t0 = time.perf_counter()
+    b = Batch(circs, dev)
+    cfg = None
+    if autotune:
+        cache = os.path.join(tempfile.gettempdir(), "qse_batch_autotune.json")
+        b.run(params)
+        cfg = b.autotune(cache)
+    t_setup = time.perf_counter() - t0
+    local = dev.index
+    p_t = torch.tensor(params, dtype=torch.float64, device=f"cuda:{local}")
+    v_t = torch.zeros(len(circs), dtype=torch.float64, device=f"cuda:{local}")
+    g_t = torch.zeros(params.size, dtype=torch.float64, device=f"cuda:{local}")
+    torch.cuda.synchronize()
+    for _ in range(warmup):
+        b.run_device(p_t.data_ptr(), v_t.data_ptr(), g_t.data_ptr())
+    dev.synchronize()
+    ms = C.c_float()
+    L.check(L.lib.qse_ctx_record(dev.handle, 8))
+    for _ in range(steps):
+        b.run_device(p_t.data_ptr(), v_t.data_ptr(), g_t.data_ptr())
+    L.check(L.lib.qse_ctx_record(dev.handle, 9))
+    L.check(L.lib.qse_ctx_elapsed(dev.handle, 8, 9, C.byref(ms)))
+    run_ms = ms.value / steps
+    st = b.stats()
+    # end to end: host parameters in, host values + gradients out
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        vals, grads = b.run(params)
+    e2e_ms = (time.perf_counter() - t0) / steps * 1e3
+
+    # accuracy: the single-state adjoint path on a few circuits of the batch
+    off = np.concatenate([[0], np.cumsum([c[2] for c in circs])])
+    diffs = []
+    for i in range(0, len(circs), max(1, len(circs) // 8)):
+        w, ops, npar, obs_t = circs[i]
+        obs, keep = L.observable(*obs_t)
+        sv = StateVector(w, dev)
+        pp = np.ascontiguousarray(params[off[i]:off[i + 1]])
+        g = np.zeros(npar)
+        v = C.c_double()
+        L.check(L.lib.qse_adjoint(sv.handle, L.dptr(ops), len(ops), pp.ctypes.data_as(L._pd), npar, C.byref(obs),
+                                  C.byref(v), g.ctypes.data_as(L._pd)))
+        diffs.append(max(abs(v.value - vals[i]), float(np.max(np.abs(g - grads[off[i]:off[i + 1]])))))
+        del sv
+
+    # plain-kernel parameter shift: per width, one circuit's execute + <O>, scaled by depth
+    dev.set_fusion(False)
+    per_width = {}
+    v = C.c_double()
+    for i, (w, ops, npar, obs_t) in enumerate(circs):
+        if w in per_width:
+            continue
+        obs, keep = L.observable(*obs_t)
+        sv = StateVector(w, dev)
+        bound = ops.copy()
+        pp = params[off[i]:off[i + 1]]
+        for j in range(len(bound)):
+            if int(bound[j]["param"]) >= 0:
+                bound[j]["theta"] = bound[j]["theta"] + bound[j]["coeff"] * pp[int(bound[j]["param"])]
+                bound[j]["param"] = -1
+
+        def f_at():
+            L.check(L.lib.qse_state_reset(sv.handle))
+            L.check(L.lib.qse_execute(sv.handle, L.dptr(bound), len(bound), None, 0, None, None, 0, None))
+            L.check(L.lib.qse_expectation(sv.handle, C.byref(obs), C.byref(v)))
+
+        f_at()
+        t0 = time.perf_counter()
+        for _ in range(3):
+            f_at()
+        per_width[w] = ((time.perf_counter() - t0) / 3, len(ops))
+        del sv
+    dev.set_fusion(True, 12, 0)
+    ps_total = 0.0
+    occ_total = 0
+    for (w, ops, npar, obs_t) in circs:
+        t, g0 = per_width[w]
+        occ = int(np.sum(ops["param"] >= 0))
+        occ_total += occ
+        ps_total += 2 * occ * t * len(ops) / g0
+    hbm_peak, peak_kind = peaks()
+    hbm_gbs = st["hbm_bytes"] / (run_ms / 1e3) / 1e9
+    return {
+        "workload": f"{count} HEA circuits, width U{{10..22}}, depth U{{4..12}} (RY+RZ per qubit + CNOT ring), "
+                    f"sum_i Z_i; {params.size} parameters, {occ_total} parameterised occurrences",
+        "circuits_per_s": len(circs) / (run_ms / 1e3),
+        "gradient_entries_per_s": params.size / (run_ms / 1e3),
+        "run_ms": run_ms,
+        "e2e_ms": e2e_ms,
+        "e2e_circuits_per_s": len(circs) / (e2e_ms / 1e3),
+        "param_shift_plain_ms_est": ps_total * 1e3,
+        "adjoint_batch_vs_plain_param_shift": ps_total / (run_ms / 1e3),
+        "max_abs_diff_vs_single_state_adjoint": max(diffs),
+        "config": None if cfg is None else cfg.__dict__,
+        "stats": {k: st[k] for k in ("passes", "items", "tile_visits", "hbm_bytes", "grid", "smem_bytes", "plan_ms")},
+        "hbm_gbs_multi_tile": hbm_gbs,
+        "hbm_frac_multi_tile": hbm_gbs / hbm_peak,
+        "setup_s": t_setup,
+        "timing": "device: CUDA events on the library stream around `steps` graph replays (device params); "
+                  "e2e: host wall clock of qse_batch_run (params H2D, values+grads D2H); plain param-shift: "
+                  "host wall clock of plain-kernel execute+<O> per width, scaled by depth and occurrences",
     }
 
 

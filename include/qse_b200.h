@@ -298,6 +298,9 @@ typedef struct qse_batch_config {
     uint32_t chain_tiles;   /* circuits with at most this many tiles per pass run as one
                                work item (one CTA, start to end); >= 1                    */
     uint32_t ctas_per_sm;   /* persistent CTAs per SM, 0 = as many as fit                 */
+    uint32_t grad_slots;    /* gradient slots per pass, 0 = no cap                        */
+    uint32_t wide_regs;     /* 1: up to 255 registers per thread (threads <= 256, one CTA
+                               per SM); 0: 128 registers (two CTAs of 256 per SM)         */
 } qse_batch_config;
 QSE_API int qse_batch_set_config(qse_batch* b, const qse_batch_config* cfg);
 QSE_API int qse_batch_get_config(const qse_batch* b, qse_batch_config* cfg);

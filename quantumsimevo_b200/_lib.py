@@ -56,7 +56,8 @@ class QseBatchCircuit(C.Structure):
 
 class QseBatchConfig(C.Structure):
     _fields_ = [("threads", C.c_uint32), ("reg_bits", C.c_uint32), ("max_gates", C.c_uint32),
-                ("chain_tiles", C.c_uint32), ("ctas_per_sm", C.c_uint32)]
+                ("chain_tiles", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("grad_slots", C.c_uint32),
+                ("wide_regs", C.c_uint32)]
 
 
 class QseBatchStats(C.Structure):

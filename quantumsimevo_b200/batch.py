@@ -27,6 +27,8 @@ class BatchConfig:
     max_gates: int = 0      # non-diagonal gates per pass, 0 = no cap
     chain_tiles: int = 1    # circuits with <= this many tiles run start to end in one CTA
     ctas_per_sm: int = 0    # 0 = as many as fit
+    grad_slots: int = 0     # gradient slots per pass, 0 = no cap
+    wide_regs: int = 0      # 1: up to 255 registers per thread (threads <= 256); 0: 128
 
 
 class Batch:
@@ -70,11 +72,13 @@ class Batch:
     def config(self) -> BatchConfig:
         c = L.QseBatchConfig()
         check(lib.qse_batch_get_config(self.handle, C.byref(c)))
-        return BatchConfig(c.threads, c.reg_bits, c.max_gates, c.chain_tiles, c.ctas_per_sm)
+        return BatchConfig(c.threads, c.reg_bits, c.max_gates, c.chain_tiles, c.ctas_per_sm, c.grad_slots,
+                           c.wide_regs)
 
     @config.setter
     def config(self, cfg: BatchConfig) -> None:
-        c = L.QseBatchConfig(cfg.threads, cfg.reg_bits, cfg.max_gates, cfg.chain_tiles, cfg.ctas_per_sm)
+        c = L.QseBatchConfig(cfg.threads, cfg.reg_bits, cfg.max_gates, cfg.chain_tiles, cfg.ctas_per_sm,
+                             cfg.grad_slots, cfg.wide_regs)
         check(lib.qse_batch_set_config(self.handle, C.byref(c)))
 
     def autotune(self, cache_path: str | None = None) -> BatchConfig:

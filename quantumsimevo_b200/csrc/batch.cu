@@ -120,6 +120,7 @@ struct BatchArgs {
 
 constexpr uint32_t kMaxThreads = 512;
 
+// exchange buffer | group values | per-warp gradient partials | warp sums
 size_t smem_bytes(uint32_t kmax, uint32_t max_groups, uint32_t max_slots, uint32_t threads)
 {
     const size_t nwarps = threads / 32;
@@ -216,7 +217,8 @@ __device__ __forceinline__ void run_tile(const BatchArgs& A, uint32_t pid, uint3
         }
     }
 
-    OpsEnv E{A.ops + P.op0, P.nops, A.layouts + P.lay0, A.mats + 8 * size_t(P.mat0), s_tile, k, obase, xbuf, gval, wpart, nwarps};
+    const OpsEnv E{A.ops + P.op0, P.nops, A.layouts + P.lay0, A.mats + 8 * size_t(P.mat0), s_tile, k, obase,
+                   xbuf, gval, wpart, nwarps};
     run_ops<RB, 2>(E, L, a, rev ? 2 : 1, active);
 
     if (!(flags & F_NOSTORE) && active) {
@@ -242,8 +244,11 @@ __device__ __forceinline__ void run_tile(const BatchArgs& A, uint32_t pid, uint3
     }
 }
 
-template <int RB>
-__global__ void __launch_bounds__(kMaxThreads, 1) k_batch(const __grid_constant__ BatchArgs A)
+// Register budget: WIDE = 0 caps the kernel at 128 registers per thread (two
+// CTAs of 256 threads per SM, a few spills); WIDE = 1 lets it use up to 255
+// (CTAs of at most 256 threads, one per SM).  The autotuner picks by measurement.
+template <int RB, int WIDE>
+__global__ void __launch_bounds__(WIDE ? 256 : kMaxThreads, 1) k_batch(const __grid_constant__ BatchArgs A)
 {
     extern __shared__ double2 smem[];
     const uint32_t tid = threadIdx.x;
@@ -344,7 +349,15 @@ __global__ void k_fin_out(const uint32_t* __restrict__ csr, const uint32_t* __re
 // ------------------------------------------------------------------ host
 struct Config {
     uint32_t threads = 256, rb = 3, max_gates = 0, chain_tiles = 1, ctas_per_sm = 0;
+    uint32_t grad_slots = 0;   // gradient slots per pass, 0 = no cap
+    uint32_t wide = 0;         // 1: up to 255 registers per thread (threads <= 256); 0: 128
 };
+
+const void* kernel_of(const Config& c)
+{
+    if (c.rb == 3) return c.wide ? reinterpret_cast<const void*>(k_batch<3, 1>) : reinterpret_cast<const void*>(k_batch<3, 0>);
+    return c.wide ? reinterpret_cast<const void*>(k_batch<2, 1>) : reinterpret_cast<const void*>(k_batch<2, 0>);
+}
 
 struct CircuitHost {
     uint32_t w = 0;
@@ -503,6 +516,8 @@ void build(qse_batch* b)
         opt.max_gates = cf.max_gates;
         opt.max_terms = 512;
         opt.keep_gphase = false;
+        opt.direct_phases = true;
+        opt.max_slots = cf.grad_slots;
         uint32_t perm0[64];
         for (uint32_t q = 0; q < 64; ++q) perm0[q] = q;
 
@@ -667,7 +682,7 @@ void build(qse_batch* b)
     if (smem + 64 > ctx->smem_optin)
         fail(QSE_ERR_SIZE, "batch: a pass needs " + std::to_string(smem) +
                                " B of shared memory; lower max_gates or the tile size");
-    const void* kfn = cf.rb == 3 ? reinterpret_cast<const void*>(k_batch<3>) : reinterpret_cast<const void*>(k_batch<2>);
+    const void* kfn = kernel_of(cf);
     {
         cudaFuncAttributes fa{};
         QSE_CUDA(cudaFuncGetAttributes(&fa, kfn));
@@ -787,8 +802,11 @@ void enqueue(qse_batch* b)
         QSE_CUDA(cudaGetLastError());
     }
     if (b->args.nitems) {
-        if (b->cfg.rb == 3) k_batch<3><<<b->grid, b->cfg.threads, b->smem, s>>>(b->args);
-        else k_batch<2><<<b->grid, b->cfg.threads, b->smem, s>>>(b->args);
+        const Config& c = b->cfg;
+        if (c.rb == 3 && c.wide) k_batch<3, 1><<<b->grid, c.threads, b->smem, s>>>(b->args);
+        else if (c.rb == 3) k_batch<3, 0><<<b->grid, c.threads, b->smem, s>>>(b->args);
+        else if (c.wide) k_batch<2, 1><<<b->grid, c.threads, b->smem, s>>>(b->args);
+        else k_batch<2, 0><<<b->grid, c.threads, b->smem, s>>>(b->args);
         QSE_CUDA(cudaGetLastError());
     }
     if (b->nfins) {
@@ -884,7 +902,8 @@ std::string config_json(const Config& c)
 {
     std::ostringstream os;
     os << "{\"threads\":" << c.threads << ",\"reg_bits\":" << c.rb << ",\"max_gates\":" << c.max_gates
-       << ",\"chain_tiles\":" << c.chain_tiles << ",\"ctas_per_sm\":" << c.ctas_per_sm << "}";
+       << ",\"chain_tiles\":" << c.chain_tiles << ",\"ctas_per_sm\":" << c.ctas_per_sm
+       << ",\"grad_slots\":" << c.grad_slots << ",\"wide_regs\":" << c.wide << "}";
     return os.str();
 }
 
@@ -928,7 +947,8 @@ bool parse_config(const std::string& s, Config& c)
     };
     Config t;
     bool ok = get("threads", t.threads) && get("reg_bits", t.rb) && get("max_gates", t.max_gates) &&
-              get("chain_tiles", t.chain_tiles) && get("ctas_per_sm", t.ctas_per_sm);
+              get("chain_tiles", t.chain_tiles) && get("ctas_per_sm", t.ctas_per_sm) &&
+              get("grad_slots", t.grad_slots) && get("wide_regs", t.wide);
     if (ok) c = t;
     return ok;
 }
@@ -937,6 +957,9 @@ void validate(const qse_batch* b, const Config& c)
 {
     if (c.threads < 32 || c.threads > kMaxThreads || (c.threads & (c.threads - 1)))
         fail(QSE_ERR_INVALID, "batch: threads must be a power of two in 32..512");
+    if (c.wide > 1 || (c.wide && c.threads > 256))
+        fail(QSE_ERR_INVALID, "batch: wide_regs needs threads <= 256");
+    if (c.grad_slots > 4096) fail(QSE_ERR_INVALID, "batch: grad_slots too large");
     if (c.rb != 2 && c.rb != 3) fail(QSE_ERR_INVALID, "batch: reg_bits must be 2 or 3");
     if (c.chain_tiles < 1) fail(QSE_ERR_INVALID, "batch: chain_tiles must be >= 1");
     for (const CircuitHost& ch : b->circs)
@@ -1111,6 +1134,8 @@ int qse_batch_set_config(qse_batch* b, const qse_batch_config* cfg)
     c.max_gates = cfg->max_gates;
     c.chain_tiles = cfg->chain_tiles;
     c.ctas_per_sm = cfg->ctas_per_sm;
+    c.grad_slots = cfg->grad_slots;
+    c.wide = cfg->wide_regs;
     validate(b, c);
     QSE_CUDA(cudaSetDevice(b->ctx->device));
     QSE_CUDA(cudaStreamSynchronize(b->ctx->stream));
@@ -1129,6 +1154,8 @@ int qse_batch_get_config(const qse_batch* b, qse_batch_config* cfg)
     cfg->max_gates = b->cfg.max_gates;
     cfg->chain_tiles = b->cfg.chain_tiles;
     cfg->ctas_per_sm = b->cfg.ctas_per_sm;
+    cfg->grad_slots = b->cfg.grad_slots;
+    cfg->wide_regs = b->cfg.wide;
     QSE_BATCH_GUARD_END
 }
 
@@ -1168,13 +1195,16 @@ int qse_batch_autotune(qse_batch* b, const char* cache_path)
     }
     uint32_t wmin = 64;
     for (const CircuitHost& ch : b->circs) wmin = std::min(wmin, ch.w);
-    // block shape x tile qubits, then gates fused per pass, then single-CTA threshold
+    // block shape x tile qubits x register budget, then gates fused per pass, then
+    // the single-CTA threshold
     std::vector<Config> shapes;
-    const uint32_t shape_list[][2] = {{128, 3}, {256, 3}, {512, 3}, {256, 2}, {512, 2}};
-    for (auto& s : shape_list) {
+    const uint32_t shape_list[][3] = {{128, 3, 0}, {256, 3, 0}, {512, 3, 0}, {256, 2, 0}, {512, 2, 0},
+                                      {256, 3, 1}};
+    for (auto& sh : shape_list) {
         Config t;
-        t.threads = s[0];
-        t.rb = s[1];
+        t.threads = sh[0];
+        t.rb = sh[1];
+        t.wide = sh[2];
         if (wmin < t.rb + 1) continue;
         shapes.push_back(t);
     }
@@ -1197,7 +1227,7 @@ int qse_batch_autotune(qse_batch* b, const char* cache_path)
     };
     for (const Config& t : shapes) trial(t);
     {
-        Config base = best_c;
+        const Config base = best_c;
         for (uint32_t mg : {24u, 48u}) {
             Config t = base;
             t.max_gates = mg;
@@ -1205,7 +1235,7 @@ int qse_batch_autotune(qse_batch* b, const char* cache_path)
         }
     }
     {
-        Config base = best_c;
+        const Config base = best_c;
         for (uint32_t ct : {4u, 16u}) {
             Config t = base;
             t.chain_tiles = ct;

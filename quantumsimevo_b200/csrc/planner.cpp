@@ -320,6 +320,7 @@ private:
         LayoutRec rec{};
         for (uint32_t i = 0; i < P.rb; ++i) rec.reg[i] = uint8_t(reg_[i]);
         rec.nthr = uint8_t(nthr_);
+        for (int t = 0; t < nthr_; ++t) rec.thr[t] = uint8_t(thr_[t]);
         uint32_t s[16] = {0};
         if (prev && nthr_ >= 3) {
             int pl[3], nl[3], np = 0;
@@ -394,7 +395,12 @@ private:
         uint64_t oc;
         split(sup, f, tc, oc);
         int nreg = popc(f);
-        int kind = nreg == 0 ? K_ACC_THR : (nreg == 1 ? K_ACC_REG : K_PHD);
+        // direct_phases: terms on register bits whose angle does not depend on
+        // the thread (no thread condition) are direct, their group's sum turned
+        // into (cos, sin) once per CTA; otherwise single-bit terms accumulate
+        // angles per thread, one sincos per flush.
+        const bool direct1 = opt_.direct_phases && tc == 0;
+        int kind = nreg == 0 ? K_ACC_THR : ((nreg == 1 && !direct1) ? K_ACC_REG : K_PHD);
         int key2 = kind == K_ACC_REG ? __builtin_ctz(f) : (kind == K_PHD ? f : 0);
         auto key = std::make_tuple(kind, key2, int(tc));
         auto it = open_.find(key);
@@ -549,12 +555,14 @@ Plan build(const std::vector<Gate>& gates, uint32_t n, const uint32_t* perm_in, 
         uint64_t bN = 0, bD = 0;
         std::vector<Absorbed> abs;
         std::vector<size_t> deferred;
-        uint32_t nN = 0, nterms = 0;
+        uint32_t nN = 0, nterms = 0, nslots = 0;
         double gph = 0.0;
         for (size_t idx : remaining) {
             const Info& in = info[idx];
             const Gate& g = gates[idx];
             bool blocked = ((in.nset | in.dset) & bN) || (in.nset & bD);
+            const bool slot = opt.grads && g.grad >= 0 && in.cls != C_SWAP;
+            if (slot && opt.max_slots && nslots >= opt.max_slots) blocked = true;
             if (!blocked) {
                 if (in.cls == C_SWAP) {
                     std::swap(perm[g.t], perm[g.c]);
@@ -568,6 +576,7 @@ Plan build(const std::vector<Gate>& gates, uint32_t n, const uint32_t* perm_in, 
                         abs.push_back(Absorbed{idx, &g, C_DIAG, perm[g.t],
                                                g.type == QSE_GATE_CPHASE ? perm[g.c] : 0u, ps});
                         ++nterms;
+                        nslots += slot ? 1 : 0;
                         continue;
                     }
                 } else {
@@ -578,6 +587,7 @@ Plan build(const std::vector<Gate>& gates, uint32_t n, const uint32_t* perm_in, 
                         T |= pt;
                         abs.push_back(Absorbed{idx, &g, in.cls, perm[g.t], in.cls == C_CX ? perm[g.c] : 0, 0});
                         ++nN;
+                        nslots += slot ? 1 : 0;
                         continue;
                     }
                 }

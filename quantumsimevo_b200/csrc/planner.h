@@ -59,8 +59,9 @@ struct LayoutRec {
     uint8_t nthr;      // number of thread-index bits
     uint8_t pad[3];
     uint16_t L[16];    // shared-memory slot image of every tile-local bit (XOR-linear map)
+    uint8_t thr[16];   // tile-local bit of thread-index bit t (ascending), t < nthr
 };
-static_assert(sizeof(LayoutRec) == 40, "LayoutRec layout");
+static_assert(sizeof(LayoutRec) == 56, "LayoutRec layout");
 
 struct TermRec {       // one diagonal term: angle theta if all outer bits of ocond are set
     uint64_t ocond;
@@ -124,6 +125,9 @@ struct Options {
     uint32_t max_gates = 0;      // 0 = no cap on non-diagonal gates per pass
     uint32_t max_terms = 1024;   // diagonal terms per pass (shared-memory group table)
     bool grads = false;          // emit K_GRAD_* for gates with grad >= 0
+    uint32_t max_slots = 0;      // gradient slots per pass, 0 = no cap
+    bool direct_phases = false;  // single-register-bit phase terms without a thread
+                                 // condition as direct (cos, sin) groups
     bool keep_gphase = true;     // false: drop RZ's global phase (expectations and gradients
                                  // do not see it; the pass programs then depend on angles
                                  // only through op_angles / term_angles)

@@ -145,8 +145,10 @@ template <int RB>
 __device__ __forceinline__ void phase_masked(int f, double2 (&a)[1 << RB], double2 e)
 {
     constexpr int R = 1 << RB;
-    // f has at least two bits (single-bit phases go through the accumulators)
     switch (f) {
+    case 1: phase_pattern<R, 1>(a, e); break;
+    case 2: phase_pattern<R, 2>(a, e); break;
+    case 4: phase_pattern<R, 4>(a, e); break;
     case 3: phase_pattern<R, 3>(a, e); break;
     case 5: phase_pattern<R, 5>(a, e); break;
     case 6: phase_pattern<R, 6>(a, e); break;
@@ -154,6 +156,7 @@ __device__ __forceinline__ void phase_masked(int f, double2 (&a)[1 << RB], doubl
     default:
         if constexpr (RB > 3) {
             switch (f) {
+            case 8: phase_pattern<R, 8>(a, e); break;
             case 9: phase_pattern<R, 9>(a, e); break;
             case 10: phase_pattern<R, 10>(a, e); break;
             case 11: phase_pattern<R, 11>(a, e); break;
@@ -188,49 +191,39 @@ __device__ __forceinline__ double warp_sum(double v)
 
 template <int RB>
 struct LayoutState {
-    int reg[RB];        // tile-local bits in registers
-    uint64_t rg[RB];    // their physical masks
-    uint64_t gbase;     // physical index of register 0 of this thread
+    int reg[RB];                     // tile-local bits in registers
+    uint64_t rg[RB];                 // their physical masks
+    uint64_t gbase;                  // physical index of register 0 of this thread
+    const plan::LayoutRec* rec;      // thread-bit list of the layout
 };
 
 template <int RB>
 __device__ __forceinline__ void load_layout(LayoutState<RB>& L, const plan::LayoutRec* rec, const uint8_t* tphys,
-                                            uint32_t k, uint64_t obase, uint32_t tid)
+                                            uint32_t /*k*/, uint64_t obase, uint32_t tid)
 {
+    L.rec = rec;
 #pragma unroll
     for (int i = 0; i < RB; ++i) {
         L.reg[i] = rec->reg[i];
         L.rg[i] = uint64_t(1) << tphys[L.reg[i]];
     }
     uint64_t g = obase;
-    uint32_t t = 0;
-    for (uint32_t b = 0; b < k; ++b) {
-        bool isreg = false;
-#pragma unroll
-        for (int i = 0; i < RB; ++i) isreg |= (L.reg[i] == int(b));
-        if (!isreg) {
-            if ((tid >> t) & 1u) g |= uint64_t(1) << tphys[b];
-            ++t;
-        }
-    }
+    const uint32_t nthr = rec->nthr;
+    for (uint32_t t = 0; t < nthr; ++t)
+        if ((tid >> t) & 1u) g |= uint64_t(1) << tphys[rec->thr[t]];
     L.gbase = g;
 }
 
 // shared-memory slot of register 0 and per-register-bit slot images under map Lm
 template <int RB>
-__device__ __forceinline__ uint32_t slot_base(const LayoutState<RB>& L, const uint16_t* Lm, uint32_t k, uint32_t tid,
-                                              uint32_t (&sreg)[RB])
+__device__ __forceinline__ uint32_t slot_base(const LayoutState<RB>& L, const uint16_t* Lm, uint32_t /*k*/,
+                                              uint32_t tid, uint32_t (&sreg)[RB])
 {
-    uint32_t sb = 0, t = 0;
-    for (uint32_t b = 0; b < k; ++b) {
-        bool isreg = false;
-#pragma unroll
-        for (int i = 0; i < RB; ++i) isreg |= (L.reg[i] == int(b));
-        if (!isreg) {
-            if ((tid >> t) & 1u) sb ^= Lm[b];
-            ++t;
-        }
-    }
+    uint32_t sb = 0;
+    const plan::LayoutRec* r = L.rec;
+    const uint32_t nthr = r->nthr;
+    for (uint32_t t = 0; t < nthr; ++t)
+        if ((tid >> t) & 1u) sb ^= Lm[r->thr[t]];
 #pragma unroll
     for (int i = 0; i < RB; ++i) sreg[i] = Lm[L.reg[i]];
     return sb;
@@ -341,8 +334,10 @@ __device__ __forceinline__ void run_ops(const OpsEnv& E, LayoutState<RB>& L, dou
 #pragma unroll
     for (int i = 0; i < RB; ++i) acc[i] = 0.0;
 
+    KOp nxt = E.nops ? E.ops[0] : KOp{};
     for (uint32_t i = 0; i < E.nops; ++i) {
-        const KOp op = E.ops[i];
+        const KOp op = nxt;
+        if (i + 1 < E.nops) nxt = E.ops[i + 1];  // in flight while this op executes
         const bool tc = (tid & op.tcond) == op.tcond;
         switch (op.kind) {
         case plan::K_H: {
