@@ -20,6 +20,11 @@ cpu_baseline / --impl reference
 qaoa       adjoint gradients/s (24-qubit 3-regular Max-Cut, p=8, 16 params)
            vs the parameter-shift rule with one kernel per gate, and the max
            difference between the two gradients.
+batch      512 parameterised circuits (widths 10..22): forward <O> and the full
+           adjoint gradient of each, one persistent kernel per run replayed as
+           a CUDA graph, against parameter shift with one kernel per gate.
+           --batch-only runs just this section (--batch-circuits/-wmin/-wmax
+           set a smaller case, --no-autotune keeps the default configuration).
 Multi-GPU: the state does not shard here; every rank runs its own replica
 (weak scaling), value = sum over ranks.
 """
@@ -54,6 +59,11 @@ def parse():
     ap.add_argument("--shots", type=int, default=SHOTS)
     ap.add_argument("--no-qaoa", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-only", action="store_true", help="only the batched forward+adjoint section")
+    ap.add_argument("--batch-circuits", type=int, default=512)
+    ap.add_argument("--batch-wmin", type=int, default=10)
+    ap.add_argument("--batch-wmax", type=int, default=22)
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-gates", type=int, default=0, help="gates in the CPU sample (0 = auto)")
     ap.add_argument("--tile", type=int, default=0, help="tile qubits of the fused passes (0 = library default)")
@@ -220,6 +230,14 @@ def main():
     from quantumsimevo_b200 import workloads as W
     from quantumsimevo_b200.circuit import Circuit, Device, StateVector
 
+    if args.batch_only:
+        if rank == 0:
+            r = bench_batch(Device(local), L, W, np, steps=args.steps, warmup=args.warmup,
+                            autotune=not args.no_autotune, count=args.batch_circuits, wmin=args.batch_wmin,
+                            wmax=args.batch_wmax)
+            print(json.dumps(r))
+        return
+
     n = args.qubits
     ops = W.hrz_qft(n, seed=2)
     ngates = len(ops)
@@ -302,12 +320,15 @@ def main():
     bytes_per_pass = 32.0 * (1 << n)
     avg_pass_ms = pass_ms / max(1, pass_launches)
     achieved = bytes_per_pass / (avg_pass_ms / 1e3) / 1e9
+    # DRAM bytes per launch from the committed ncu summary (26-qubit capture
+    # scaled by the amplitudes per launch), for the 30-qubit workload only
     traffic = None
     try:
-        with open(os.path.join(ROOT, "profiles", "tile_pass_traffic.json")) as f:
-            tr = json.load(f)
-        traffic = tr.get(f"{n}q_bytes_per_launch")
-    except Exception:
+        with open(os.path.join(ROOT, "profiles", "qse_pass_hrz_qft_26q.md")) as f:
+            for line in f:
+                if f"traffic_bytes_per_launch_{n}q:" in line:
+                    traffic = float(line.split(":")[-1])
+    except OSError:
         pass
 
     # ---- timed: end to end through the public API (host buffers) ----
@@ -350,7 +371,8 @@ def main():
         qaoa = bench_qaoa(dev, L, W, np)
     batch = None
     if rank == 0 and not args.no_batch:
-        batch = bench_batch(dev, L, W, np, steps=args.steps, warmup=args.warmup)
+        batch = bench_batch(dev, L, W, np, steps=args.steps, warmup=args.warmup, autotune=not args.no_autotune,
+                            count=args.batch_circuits, wmin=args.batch_wmin, wmax=args.batch_wmax)
 
     barrier()
     if rank == 0:
@@ -368,7 +390,7 @@ def main():
             "hbm_gbs_execute": bytes_per_pass * passes_per_exec / (pass_ms / args.steps / 1e3) / 1e9,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "k_tile<4,1> (fused pass)", "bytes_per_launch": bytes_per_pass,
+                         "kernel": "qse_pass (fused pass, NVRTC-specialised)", "bytes_per_launch": bytes_per_pass,
                          "avg_launch_ms": avg_pass_ms},
             "e2e": {"value": e2e_value, "unit": "gates/s", "h2d_bytes_per_step": int(ops.nbytes),
                     "d2h_bytes_per_step": int(8 * args.shots + 8)},
@@ -457,7 +479,7 @@ def bench_qaoa(dev, L, W, np):
     }
 
 
-def bench_batch(dev, L, W, np, steps=5, warmup=3, autotune=True, count=512):
+def bench_batch(dev, L, W, np, steps=5, warmup=3, autotune=True, count=512, wmin=10, wmax=22):
     """512 hardware-efficient-ansatz circuits (width U{10..22}, depth U{4..12}
     layers of RY+RZ per qubit and a CNOT ring, observable sum_i Z_i): forward
     <O> and the full adjoint gradient of every circuit per run, one persistent
@@ -468,7 +490,7 @@ def bench_batch(dev, L, W, np, steps=5, warmup=3, autotune=True, count=512):
 
     from quantumsimevo_b200.batch import Batch
     from quantumsimevo_b200.circuit import StateVector
-    hb = W.hea_batch(count, 10, 22, 4, 12, seed=5)
+    hb = W.hea_batch(count, wmin, wmax, 4, 12, seed=5)
     circs = [(w, ops, len(p), obs) for (w, ops, p, obs) in hb]
     params = np.concatenate([p for (_, _, p, _) in hb])
     t0 = time.perf_counter()
@@ -554,7 +576,7 @@ def bench_batch(dev, L, W, np, steps=5, warmup=3, autotune=True, count=512):
     hbm_peak, peak_kind = peaks()
     hbm_gbs = st["hbm_bytes"] / (run_ms / 1e3) / 1e9
     return {
-        "workload": f"{count} HEA circuits, width U{{10..22}}, depth U{{4..12}} (RY+RZ per qubit + CNOT ring), "
+        "workload": f"{count} HEA circuits, width U{{{wmin}..{wmax}}}, depth U{{4..12}} (RY+RZ per qubit + CNOT ring), "
                     f"sum_i Z_i; {params.size} parameters, {occ_total} parameterised occurrences",
         "circuits_per_s": len(circs) / (run_ms / 1e3),
         "gradient_entries_per_s": params.size / (run_ms / 1e3),
