@@ -537,6 +537,7 @@ int qse_plan_compile(uint32_t nqubits, const qse_op* ops, size_t nops, const dou
     opt.rb = nstates == 2 ? 3 : 4;
     opt.k = std::min<uint32_t>(tile_qubits ? tile_qubits : (nstates == 2 ? 11 : 12), nqubits);
     opt.grads = nstates == 2;
+    opt.acc_mul = true;
     if (nstates == 2) {
         opt.max_terms = 512;
         opt.max_gates = 256;

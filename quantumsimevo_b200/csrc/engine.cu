@@ -277,6 +277,7 @@ void execute_program(qse_state* st, const qse_op* ops, size_t nops, const double
         opt.rb = 4;
         opt.k = tile_qubits_for(ctx, st->n, 4, 12);
         opt.max_gates = uint32_t(std::max(0, ctx->max_gates_per_pass));
+        opt.acc_mul = ctx->jit != 0;
         plan::Plan pl = plan::build(gates, st->n, st->perm, opt);
         Uploaded up = upload_plan(ctx, pl);
         PassRunner runner(st, pl, up, 1, 4);
@@ -482,6 +483,7 @@ double adjoint(qse_state* st, const qse_op* ops, size_t nops, const double* para
     opt.rb = 3;
     opt.k = tile_qubits_for(ctx, st->n, 3, 11);
     opt.grads = true;
+    opt.acc_mul = ctx->jit != 0;
     opt.max_terms = 512;
     opt.max_gates = 256;
     plan::Plan pl = plan::build(rev, st->n, st->perm, opt);

@@ -181,9 +181,26 @@ struct Gen {
 
     void emit_flush_reg(int p)
     {
-        o << "  if (ar" << p << " != 0.0) { const double2 e = expi(ar" << p << "); ar" << p << " = 0.0;";
+        if (P.acc_mul) {
+            o << "  if (notOne(ar" << p << ")) { const double2 e = ar" << p << "; ar" << p
+              << " = make_double2(1.0, 0.0);";
+        } else {
+            o << "  if (ar" << p << " != 0.0) { const double2 e = expi(ar" << p << "); ar" << p << " = 0.0;";
+        }
         for (int s = 0; s < ns; ++s) o << " phD<" << (1 << p) << ">(" << (s ? "a1" : "a0") << ", e);";
         o << " }\n";
+    }
+
+    // per-thread accumulators: angles (sincos at each flush) or, with acc_mul,
+    // complex factors multiplied by the groups' per-CTA (cos, sin)
+    void emit_acc_decls()
+    {
+        const char* ty = P.acc_mul ? "double2" : "double";
+        const char* one = P.acc_mul ? "make_double2(1.0, 0.0)" : "0.0";
+        o << "  " << ty << " at = " << one;
+        for (uint32_t i = 0; i < P.rb; ++i) o << ", ar" << i << " = " << one;
+        o << ";\n";
+        for (uint32_t i = P.rb; i < 4; ++i) o << "  " << ty << " ar" << i << " = " << one << "; (void)ar" << i << ";\n";
     }
 
     std::string run()
@@ -223,10 +240,7 @@ struct Gen {
             if (ns == 2) o << " a1[" << j << "] = lam[gb | " << hex(reg_off(j)) << "];";
             o << "\n";
         }
-        o << "  double at = 0.0";
-        for (uint32_t i = 0; i < P.rb; ++i) o << ", ar" << i << " = 0.0";
-        o << ";\n";
-        for (uint32_t i = P.rb; i < 4; ++i) o << "  double ar" << i << " = 0.0; (void)ar" << i << ";\n";
+        emit_acc_decls();
 
         for (const plan::KOp& op : P.ops) emit(op);
 
@@ -288,12 +302,14 @@ struct Gen {
             break;
         }
         case K_ACC_THR:
-            o << "  " << (op.tcond ? "if (" + cond(op.tcond, 0) + ") " : std::string()) << "at += gv[" << op.g
-              << "].x;\n";
+            o << "  " << (op.tcond ? "if (" + cond(op.tcond, 0) + ") " : std::string());
+            if (P.acc_mul) o << "at = cmul(at, gv[" << op.g << "]);\n";
+            else o << "at += gv[" << op.g << "].x;\n";
             break;
         case K_ACC_REG:
-            o << "  " << (op.tcond ? "if (" + cond(op.tcond, 0) + ") " : std::string()) << "ar" << p << " += gv["
-              << op.g << "].x;\n";
+            o << "  " << (op.tcond ? "if (" + cond(op.tcond, 0) + ") " : std::string());
+            if (P.acc_mul) o << "ar" << p << " = cmul(ar" << p << ", gv[" << op.g << "]);\n";
+            else o << "ar" << p << " += gv[" << op.g << "].x;\n";
             break;
         case K_PHD: {
             std::string t = op.tcond ? "if (" + cond(op.tcond, 0) + ") " : std::string();
@@ -307,7 +323,16 @@ struct Gen {
             for (uint32_t r = 0; r < P.rb; ++r)
                 if ((op.f >> r) & 1) emit_flush_reg(int(r));
             const bool unit = op.a == 1.0 && op.b == 0.0;
-            if (unit) {
+            if (P.acc_mul) {
+                if (unit) {
+                    o << "  if (notOne(at)) { const double2 e = at; at = make_double2(1.0, 0.0);";
+                } else {
+                    uint32_t i = push(op.a);
+                    push(op.b);
+                    o << "  { const double2 e = cmul(make_double2(P.v[" << i << "], P.v[" << i + 1
+                      << "]), at); at = make_double2(1.0, 0.0);";
+                }
+            } else if (unit) {
                 o << "  if (at != 0.0) { const double2 e = expi(at); at = 0.0;";
             } else {
                 uint32_t i = push(op.a);

@@ -431,7 +431,7 @@ private:
         GroupRec gr{};
         gr.first = uint32_t(P.terms.size());
         gr.count = uint32_t(og.terms.size());
-        gr.direct = og.kind == K_PHD ? 1u : 0u;
+        gr.direct = (og.kind == K_PHD || opt_.acc_mul) ? 1u : 0u;
         for (size_t i = 0; i < og.src.size(); ++i)
             if (og.src[i] >= 0) P.term_angles.push_back(AngleRef{uint32_t(P.terms.size() + i), uint32_t(og.src[i])});
         P.terms.insert(P.terms.end(), og.terms.begin(), og.terms.end());
@@ -601,6 +601,7 @@ Plan build(const std::vector<Gate>& gates, uint32_t n, const uint32_t* perm_in, 
         PassProgram prog;
         prog.k = k;
         prog.rb = opt.rb;
+        prog.acc_mul = opt.acc_mul;
         uint32_t b = 0;
         for (uint32_t q = 0; q < n; ++q)
             if ((T >> q) & 1) prog.tile_phys[b++] = uint8_t(q);

@@ -28,8 +28,8 @@ enum KKind : uint8_t {
     K_RX,          // [[c,-is],[-is,c]] on p, (a,b) = (c,s)
     K_RY,          // [[c,-s],[s,c]] on p
     K_U,           // generic 2x2 on p, matrix index g, controls as K_X
-    K_ACC_THR,     // if thread cond: acc_thr += group value g
-    K_ACC_REG,     // if thread cond: acc[p] += group value g
+    K_ACC_THR,     // if thread cond: acc_thr += group value g  (acc_mul: acc_thr *= (cos, sin) g)
+    K_ACC_REG,     // if thread cond: acc[p] += group value g   (acc_mul: acc[p] *= (cos, sin) g)
     K_PHD,         // if thread cond: amplitudes with (j & f) == f *= group (cos, sin) g
     K_FLUSH_REG,   // amplitudes with bit p *= e^{i acc[p]}; acc[p] = 0
     K_FLUSH_ALL,   // flush acc[p] for p in f, then all amplitudes *= e^{i acc_thr} * (a + ib)
@@ -86,6 +86,7 @@ struct AngleRef {
 struct PassProgram {
     uint32_t k = 0;                 // tile qubits
     uint32_t rb = 4;                // register bits per thread
+    bool acc_mul = false;           // accumulators carry complex factors (Options::acc_mul)
     uint64_t outer_mask = 0;        // physical qubits not in the tile
     uint8_t tile_phys[16] = {0};    // physical qubit of tile-local bit b (ascending)
     uint32_t layout0 = 0;           // layout at load time (index into layouts)
@@ -128,6 +129,9 @@ struct Options {
     uint32_t max_slots = 0;      // gradient slots per pass, 0 = no cap
     bool direct_phases = false;  // single-register-bit phase terms without a thread
                                  // condition as direct (cos, sin) groups
+    bool acc_mul = false;        // accumulator groups (K_ACC_THR / K_ACC_REG) are direct too:
+                                 // kernels multiply their (cos, sin) into per-thread complex
+                                 // factors instead of summing angles and calling sincos per flush
     bool keep_gphase = true;     // false: drop RZ's global phase (expectations and gradients
                                  // do not see it; the pass programs then depend on angles
                                  // only through op_angles / term_angles)
