@@ -27,6 +27,8 @@
 // block's values.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "philox.cuh"
 #include "qse_internal.h"
 
@@ -105,6 +107,75 @@ __device__ __forceinline__ bool elem_map(double p, int e, uint64_t& d0, uint64_t
     return true;
 }
 
+// The grid of binade e as a multiplier: q = p * 2^(52-e) is exact (a power-of-two
+// scaling whose result stays below 2^53), so one multiply, one rint and one
+// exact difference give the element map.  Binades whose multiplier is not a
+// finite double (a running sum that is still zero or subnormal) keep elem_map.
+struct Grid {
+    double scale;   // 2^(52-e)
+    double limit;   // 2^(e+1): an element this large leaves the binade by itself
+    int e;
+    int fast;
+};
+
+__device__ __forceinline__ Grid grid_of(int e)
+{
+    Grid g;
+    g.e = e;
+    g.fast = (52 - e) <= 1000 ? 1 : 0;
+    g.scale = g.fast ? ldexp(1.0, 52 - e) : 0.0;
+    g.limit = ldexp(1.0, e + 1);
+    return g;
+}
+
+// elem_map on grid g: d0 == d1 unless p / G ends in exactly one half (a tie)
+__device__ __forceinline__ bool elem_map_g(double p, const Grid& g, uint64_t& d0, uint64_t& d1)
+{
+    if (!g.fast) return elem_map(p, g.e, d0, d1);
+    if (!(p < g.limit)) { d0 = d1 = kTwo53; return false; }
+    const double q = p * g.scale;
+    const double r = rint(q);
+    const double df = q - r;               // exact (Sterbenz)
+    if (df == 0.5 || df == -0.5) {         // tie: the sum must come out even
+        const uint64_t k = uint64_t(floor(q));
+        if (k & 1) { d0 = k + 1; d1 = k; }
+        else { d0 = k; d1 = k + 1; }
+    } else {
+        d0 = d1 = uint64_t(r);
+    }
+    return true;
+}
+
+// block-wide exclusive prefix of 64-bit integers (warp shuffles, then the
+// warp totals); returns the block total.  sh: >= 2 * (kBT / 32) + 1 words.
+__device__ uint64_t block_scan_add(uint64_t v, uint64_t& excl, uint64_t* sh)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nw = blockDim.x >> 5;
+    uint64_t inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += u;
+    }
+    if (lane == 31) sh[warp] = inc;
+    __syncthreads();
+    if (tid == 0) {
+        uint64_t run = 0;
+        for (int w = 0; w < nw; ++w) {
+            const uint64_t t = sh[w];
+            sh[32 + w] = run;
+            run += t;
+        }
+        sh[64] = run;
+    }
+    __syncthreads();
+    excl = sh[32 + warp] + inc - v;
+    const uint64_t total = sh[64];
+    __syncthreads();
+    return total;
+}
+
 __device__ __forceinline__ void compose(uint64_t a0, uint64_t a1, uint64_t b0, uint64_t b1, uint64_t& r0, uint64_t& r1)
 {
     // first a, then b
@@ -160,7 +231,7 @@ __device__ void block_scan_maps(uint64_t t0, uint64_t t1, uint64_t& ex0, uint64_
 // as p[0..kEPT) per thread (element index = tid*kEPT + j), starting from the
 // exact running sum c_in.  Writes the values to out (if non-null) and returns
 // the block's final sum.  Must be called by all threads of the block.
-__device__ double block_exact(const double (&p)[kEPT], uint32_t cnt, double c_in, double* out, uint64_t* sh,
+__device__ __forceinline__ double block_exact(const double (&p)[kEPT], uint32_t cnt, double c_in, double* out, uint64_t* sh,
                               double* stage)
 {
     __shared__ double s_c;
@@ -172,40 +243,65 @@ __device__ double block_exact(const double (&p)[kEPT], uint32_t cnt, double c_in
         const int e = epoch_of(c);
         const double G = ldexp(1.0, e - 52);
         const uint64_t C = uint64_t(ldexp(c, 52 - e));
-        // this thread's fold over its elements >= pos
-        uint64_t d[kEPT][2];
-        uint64_t t0 = 0, t1 = 0;
+        const Grid g = grid_of(e);
+        // this thread's element maps over its elements >= pos (even-parity
+        // offsets kept; a tie anywhere sends the block to the general path,
+        // which recomputes both offsets)
+        uint64_t Ci[kEPT];
         int bad = kBS;
+        bool pure = true;
+        uint64_t tsum = 0;
 #pragma unroll
         for (int j = 0; j < kEPT; ++j) {
             uint32_t i = tid * kEPT + j;
             uint64_t a0 = 0, a1 = 0;
             if (i >= pos && i < cnt) {
-                if (!elem_map(p[j], e, a0, a1) && bad == kBS) bad = int(i);
+                if (!elem_map_g(p[j], g, a0, a1) && bad == kBS) bad = int(i);
             }
-            d[j][0] = a0;
-            d[j][1] = a1;
-            uint64_t r0, r1;
-            compose(t0, t1, a0, a1, r0, r1);
-            t0 = r0;
-            t1 = r1;
+            Ci[j] = a0;
+            pure = pure && a0 == a1;
+            tsum += a0;
         }
-        uint64_t ex0, ex1;
-        block_scan_maps(t0, t1, ex0, ex1, sh);
-        // running values; first index that reaches 2^53 or is flagged
-        uint64_t run0 = ex0, run1 = ex1;
         int first = bad;
-        uint64_t Ci[kEPT];
+        if (__syncthreads_and(pure)) {
+            // no ties anywhere: every map is a translation and prefixes are sums
+            uint64_t ex;
+            block_scan_add(tsum, ex, sh);
+            uint64_t run = C + ex;
 #pragma unroll
-        for (int j = 0; j < kEPT; ++j) {
-            uint64_t r0, r1;
-            compose(run0, run1, d[j][0], d[j][1], r0, r1);
-            run0 = r0;
-            run1 = r1;
-            uint64_t v = C + ((C & 1) ? run1 : run0);
-            Ci[j] = v;
-            uint32_t i = tid * kEPT + j;
-            if (i >= pos && i < cnt && v >= kTwo53 && int(i) < first) first = int(i);
+            for (int j = 0; j < kEPT; ++j) {
+                run += Ci[j];
+                Ci[j] = run;
+                uint32_t i = tid * kEPT + j;
+                if (i >= pos && i < cnt && run >= kTwo53 && int(i) < first) first = int(i);
+            }
+        } else {
+            uint64_t t0 = 0, t1 = 0;
+#pragma unroll
+            for (int j = 0; j < kEPT; ++j) {
+                uint64_t a0 = 0, a1 = 0, r0, r1;
+                const uint32_t i = tid * kEPT + j;
+                if (i >= pos && i < cnt) elem_map_g(p[j], g, a0, a1);
+                compose(t0, t1, a0, a1, r0, r1);
+                t0 = r0;
+                t1 = r1;
+            }
+            uint64_t ex0, ex1;
+            block_scan_maps(t0, t1, ex0, ex1, sh);
+            // running values; first index that reaches 2^53 or is flagged
+            uint64_t run0 = ex0, run1 = ex1;
+#pragma unroll
+            for (int j = 0; j < kEPT; ++j) {
+                uint64_t a0 = 0, a1 = 0, r0, r1;
+                const uint32_t i = tid * kEPT + j;
+                if (i >= pos && i < cnt) elem_map_g(p[j], g, a0, a1);
+                compose(run0, run1, a0, a1, r0, r1);
+                run0 = r0;
+                run1 = r1;
+                uint64_t v = C + ((C & 1) ? run1 : run0);
+                Ci[j] = v;
+                if (i >= pos && i < cnt && v >= kTwo53 && int(i) < first) first = int(i);
+            }
         }
         if (tid == 0) s_t = int(cnt);
         __syncthreads();
@@ -303,18 +399,25 @@ __global__ void __launch_bounds__(kBT) k_prob_identity(const double2* __restrict
 // amplitudes spanned by 12 physical bits S that contain physical bits 0..4
 // (contiguous 512-byte reads) and the physical images of logical bits 0..6
 // (contiguous 1 KiB writes of probabilities), and transposes through shared
-// memory.
+// memory.  Slot of read-order index r: XOR of img[b] over the set bits b of r,
+// img[b] = 2^b with a host-chosen low nibble for b >= 4, so that both the
+// write side (lanes vary r's bits 0..4) and the read side (lanes vary the
+// read-order images of logical bits 0..4) touch 16 distinct 8-byte bank pairs
+// per half-warp.  Each warp's 32 written probabilities share one 4096-block of
+// the logical array; their sum goes to that block's approximate sum (atomic:
+// only the binade guess reads it).
 struct GatherPlan {
     uint64_t outer_mask;      // physical bits outside S
     uint8_t sphys[12];        // S ascending (tile order for the reads)
     uint8_t slog[12];         // logical images of S, ascending (tile order for the writes)
     uint8_t wsrc[12];         // write-order bit b' -> read-order bit
     uint8_t pad[4];
+    uint16_t img[12];         // shared-memory slot image of read-order bit b
     uint8_t inv[64];          // physical bit -> logical bit
 };
 
 __global__ void __launch_bounds__(kBT) k_prob_gather(const double2* __restrict__ amp, double* __restrict__ prob,
-                                                     GatherPlan g)
+                                                     double* __restrict__ bsum, const __grid_constant__ GatherPlan g)
 {
     __shared__ double sm[kBS];
     const uint32_t t = threadIdx.x;
@@ -332,20 +435,25 @@ __global__ void __launch_bounds__(kBT) k_prob_gather(const double2* __restrict__
         }
     }
     uint64_t tr = ob, tw = lb;
-    uint32_t ts = 0;
+    uint32_t sw = 0, sr = 0;
     for (int b = 0; b < 8; ++b)
         if ((t >> b) & 1) {
             tr |= uint64_t(1) << g.sphys[b];
             tw |= uint64_t(1) << g.slog[b];
-            ts |= 1u << g.wsrc[b];
+            sw ^= g.img[b];
+            sr ^= g.img[g.wsrc[b]];
         }
 #pragma unroll
     for (int j = 0; j < kEPT; ++j) {
         uint64_t off = 0;
+        uint32_t so = 0;
 #pragma unroll
         for (int b = 0; b < 4; ++b)
-            if ((j >> b) & 1) off |= uint64_t(1) << g.sphys[8 + b];
-        sm[j * kBT + t] = norm2(amp[tr | off]);
+            if ((j >> b) & 1) {
+                off |= uint64_t(1) << g.sphys[8 + b];
+                so ^= g.img[8 + b];
+            }
+        sm[sw ^ so] = norm2(amp[tr | off]);
     }
     __syncthreads();
 #pragma unroll
@@ -356,19 +464,14 @@ __global__ void __launch_bounds__(kBT) k_prob_gather(const double2* __restrict__
         for (int b = 0; b < 4; ++b)
             if ((j >> b) & 1) {
                 off |= uint64_t(1) << g.slog[8 + b];
-                so |= 1u << g.wsrc[8 + b];
+                so ^= g.img[g.wsrc[8 + b]];
             }
-        prob[tw | off] = sm[ts | so];
+        const double v = sm[sr ^ so];
+        prob[tw | off] = v;
+        double ws = v;
+        for (int o = 16; o > 0; o >>= 1) ws += __shfl_xor_sync(0xffffffffu, ws, o);
+        if ((t & 31) == 0) atomicAdd(bsum + ((tw | off) >> 12), ws);
     }
-}
-
-__global__ void __launch_bounds__(kBT) k_prob_bsum(const double* __restrict__ prob, double* __restrict__ bsum)
-{
-    const uint64_t base = uint64_t(blockIdx.x) * kBS;
-    double s = 0.0;
-#pragma unroll
-    for (int j = 0; j < kEPT; ++j) s += prob[base + j * kBT + threadIdx.x];
-    block_sum_store(s, bsum + blockIdx.x);
 }
 
 // single CTA: approximate exclusive prefix -> grid guess per block
@@ -397,7 +500,8 @@ __global__ void __launch_bounds__(1024) k_cdf_guess(const double* __restrict__ b
         double slack = hi_c * 0x1.0p-20 + 1e-300;
         int e1 = lo_c - slack > 2.2250738585072014e-308 ? ilogb(lo_c - slack) : -1022;
         int e2 = hi_c + slack > 2.2250738585072014e-308 ? ilogb(hi_c + slack) : -1022;
-        guess[b] = (e2 - e1 <= 1) ? e1 : INT32_MIN;
+        // 2 e1 + 1 when the block may reach binade e1 + 1, 2 e1 when it stays in e1
+        guess[b] = (e2 - e1 <= 1) ? 2 * e1 + (e2 - e1) : INT32_MIN;
         run = hi_c;
     }
 }
@@ -406,34 +510,53 @@ __global__ void __launch_bounds__(kBT) k_cdf_summ(const double* __restrict__ pro
                                                   const int32_t* __restrict__ guess, Summ* __restrict__ summ)
 {
     __shared__ uint64_t sh[160];
-    const int32_t e = guess[blockIdx.x];
-    if (e == INT32_MIN) {
-        if (threadIdx.x == 0) summ[blockIdx.x] = Summ{{{0, 0}, {0, 0}}, e, 0};
+    const int32_t gs = guess[blockIdx.x];
+    if (gs == INT32_MIN) {
+        if (threadIdx.x == 0) summ[blockIdx.x] = Summ{{{0, 0}, {0, 0}}, gs, 0};
         return;
     }
+    const int32_t e = gs >> 1;          // arithmetic shift: floor(gs / 2)
+    const int nbin = 1 + (gs & 1);      // binades the block may run in
     __shared__ double stage[kBT * kPad];
     double p[kEPT];
     load_block_prob(prob, uint64_t(blockIdx.x) * kBS, p, stage);
     Summ out{{{0, 0}, {0, 0}}, e, 0};
-    for (int k = 0; k < 2; ++k) {
-        uint64_t t0 = 0, t1 = 0;
+    for (int k = 0; k < nbin; ++k) {
+        const Grid g = grid_of(e + k);
         int ok = 1;
+        bool pure = true;
+        uint64_t tsum = 0;
 #pragma unroll
         for (int j = 0; j < kEPT; ++j) {
-            uint64_t a0, a1, r0, r1;
-            if (!elem_map(p[j], e + k, a0, a1)) ok = 0;
-            compose(t0, t1, a0, a1, r0, r1);
-            t0 = r0;
-            t1 = r1;
+            uint64_t a0, a1;
+            if (!elem_map_g(p[j], g, a0, a1)) ok = 0;
+            pure = pure && a0 == a1;
+            tsum += a0;
         }
-        ok = __syncthreads_and(ok);
-        uint64_t ex0, ex1;
-        block_scan_maps(t0, t1, ex0, ex1, sh);
-        uint64_t r0, r1;
-        compose(ex0, ex1, t0, t1, r0, r1);
-        out.d[k][0] = r0;
-        out.d[k][1] = r1;
-        out.ok |= ok ? (1 << k) : 0;
+        const int both = __syncthreads_and(ok) | (__syncthreads_and(pure) << 1);
+        if (!(both & 1)) continue;  // an element leaves binade e+k by itself: no fold there
+        if (both & 2) {
+            uint64_t ex;
+            const uint64_t total = block_scan_add(tsum, ex, sh);
+            out.d[k][0] = out.d[k][1] = total;
+        } else {
+            uint64_t t0 = 0, t1 = 0;
+#pragma unroll
+            for (int j = 0; j < kEPT; ++j) {
+                uint64_t a0, a1, r0, r1;
+                elem_map_g(p[j], g, a0, a1);
+                compose(t0, t1, a0, a1, r0, r1);
+                t0 = r0;
+                t1 = r1;
+            }
+            uint64_t ex0, ex1;
+            block_scan_maps(t0, t1, ex0, ex1, sh);
+            uint64_t r0, r1;
+            compose(ex0, ex1, t0, t1, r0, r1);
+            out.d[k][0] = r0;
+            out.d[k][1] = r1;
+        }
+        out.ok |= 1 << k;
     }
     if (threadIdx.x == blockDim.x - 1) summ[blockIdx.x] = out;
 }
@@ -475,7 +598,12 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double* __restrict__ pr
             const uint32_t bad = uint32_t(s_end);
             if (t >= bad) m0 = m1 = 0;
             uint64_t ex0, ex1;
-            block_scan_maps(m0, m1, ex0, ex1, sh);
+            if (__syncthreads_and(m0 == m1)) {
+                block_scan_add(m0, ex0, sh);    // translations only: the prefix is a sum
+                ex1 = ex0;
+            } else {
+                block_scan_maps(m0, m1, ex0, ex1, sh);
+            }
             const uint64_t C = c > 0.0 ? uint64_t(ldexp(c, 52 - e0)) : 0;
             const uint64_t cin_t = C + ((C & 1) ? ex1 : ex0);
             const uint64_t cout_t = cin_t + ((cin_t & 1) ? m1 : m0);
@@ -638,6 +766,35 @@ GatherPlan make_gather(const qse_state* st)
         for (int r = 0; r < 12; ++r)
             if (g.sphys[r] == phys) g.wsrc[i] = uint8_t(r);
     }
+    // slot images: read-order bits 0..3 keep their place; bits >= 4 get a low
+    // nibble chosen so that the read side's half-warp bits (the read-order
+    // images of write-order bits 0..3) span all 16 low-nibble values
+    uint32_t low[12] = {0};
+    uint64_t rng = 0x2545F4914F6CDD1Dull;
+    for (int attempt = 0; attempt < 4096; ++attempt) {
+        uint32_t cand[12] = {0};
+        for (int r = 4; r < 12; ++r) {
+            rng ^= rng << 13; rng ^= rng >> 7; rng ^= rng << 17;
+            cand[r] = attempt ? uint32_t(rng >> 60) : 0u;
+        }
+        // rank over GF(2) of the 4 read-side images
+        uint32_t basis[4] = {0, 0, 0, 0};
+        int rank = 0;
+        for (int i = 0; i < 4; ++i) {
+            const int r = g.wsrc[i];
+            uint32_t v = r < 4 ? (1u << r) : cand[r];
+            for (int k = 3; k >= 0 && v; --k)
+                if ((v >> k) & 1) {
+                    if (basis[k]) v ^= basis[k];
+                    else { basis[k] = v; ++rank; v = 0; }
+                }
+        }
+        if (rank == 4) {
+            std::copy(cand, cand + 12, low);
+            break;
+        }
+    }
+    for (int r = 0; r < 12; ++r) g.img[r] = uint16_t((1u << r) ^ low[r]);
     const uint64_t all = st->n >= 64 ? ~uint64_t(0) : ((uint64_t(1) << st->n) - 1);
     g.outer_mask = all & ~S;
     return g;
@@ -684,9 +841,9 @@ CdfView build_cdf(qse_state* st)
             count_launch(ctx);
         } else {
             GatherPlan g = make_gather(st);
-            k_prob_gather<<<unsigned(size / kBS), kBT, 0, ctx->stream>>>(amp, v.cdf, g);
-            k_prob_bsum<<<nb, kBT, 0, ctx->stream>>>(v.cdf, bsum);
-            count_launch(ctx, 2);
+            QSE_CUDA(cudaMemsetAsync(bsum, 0, size_t(nb) * 8, ctx->stream));
+            k_prob_gather<<<unsigned(size / kBS), kBT, 0, ctx->stream>>>(amp, v.cdf, bsum, g);
+            count_launch(ctx);
         }
         k_cdf_guess<<<1, 1024, 0, ctx->stream>>>(bsum, nb, guess);
         k_cdf_summ<<<nb, kBT, 0, ctx->stream>>>(v.cdf, guess, summ);
