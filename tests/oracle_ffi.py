@@ -38,6 +38,7 @@ def _load_oracle():
         "orc_philox4x32_10": ([C.POINTER(_u32), C.POINTER(_u32), C.POINTER(_u32)], None),
         "orc_philox_uniform_pair": ([_u64, _u64, _pd, _pd], None),
         "orc_noise_init": ([C.POINTER(OrcNoise), C.c_uint, C.POINTER(QseNoiseConfig)], None),
+        "orc_noise_accumulate": ([C.POINTER(OrcNoise), C.c_int, C.c_uint, _pd], C.c_int),
         "orc_execute": ([_vp, C.c_uint, _vp, _sz, _pd, C.POINTER(OrcNoise), _pd, _sz], C.c_int),
         "orc_expectation": ([_vp, C.c_uint, C.POINTER(QseObservable)], _d),
         "orc_adjoint": ([C.c_uint, _vp, _sz, _pd, _sz, C.POINTER(QseObservable), _pd], _d),
@@ -140,6 +141,16 @@ def param_shift(n, ops, params, obs):
     v = oracle.orc_param_shift(n, a.ctypes.data_as(_vp), len(a), p.ctypes.data_as(_pd), p.size, C.byref(obs),
                                g.ctypes.data_as(_pd))
     return v, g
+
+
+def noise_decisions(n, ops, cfg):
+    """Noise.cpp's per-gate draws and flip counts for a gate list, without a
+    state (the decisions depend only on the gates and the draws)."""
+    nz = OrcNoise()
+    oracle.orc_noise_init(C.byref(nz), n, C.byref(cfg))
+    for op in ops_arr(ops):
+        oracle.orc_noise_accumulate(C.byref(nz), int(op["type"]), int(op["target"]), None)
+    return list(nz.bit[:n]), list(nz.phase[:n])
 
 
 def philox_pair(seed, counter):
