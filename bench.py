@@ -231,11 +231,13 @@ def main():
     from quantumsimevo_b200.circuit import Circuit, Device, StateVector
 
     if args.batch_only:
+        r = bench_batch(Device(local), L, W, np, steps=args.steps, warmup=args.warmup,
+                        autotune=not args.no_autotune, count=args.batch_circuits, wmin=args.batch_wmin,
+                        wmax=args.batch_wmax, dist=dist)
         if rank == 0:
-            r = bench_batch(Device(local), L, W, np, steps=args.steps, warmup=args.warmup,
-                            autotune=not args.no_autotune, count=args.batch_circuits, wmin=args.batch_wmin,
-                            wmax=args.batch_wmax)
             print(json.dumps(r))
+        if dist:
+            dist.destroy_process_group()
         return
 
     n = args.qubits
@@ -367,12 +369,14 @@ def main():
 
     # ---- QAOA gradients (rank 0) ----
     qaoa = None
-    if rank == 0 and not args.no_qaoa:
+    if rank == 0 and world == 1 and not args.no_qaoa:   # a single-GPU figure, reported at N = 1
         qaoa = bench_qaoa(dev, L, W, np)
     batch = None
-    if rank == 0 and not args.no_batch:
+    if not args.no_batch and (dist or rank == 0):
+        # N ranks: the batch's circuits are split across the GPUs (no collective
+        # on the data path; one gather of the results at the end)
         batch = bench_batch(dev, L, W, np, steps=args.steps, warmup=args.warmup, autotune=not args.no_autotune,
-                            count=args.batch_circuits, wmin=args.batch_wmin, wmax=args.batch_wmax)
+                            count=args.batch_circuits, wmin=args.batch_wmin, wmax=args.batch_wmax, dist=dist)
 
     barrier()
     if rank == 0:
@@ -479,36 +483,46 @@ def bench_qaoa(dev, L, W, np):
     }
 
 
-def bench_batch(dev, L, W, np, steps=5, warmup=3, autotune=True, count=512, wmin=10, wmax=22):
+def bench_batch(dev, L, W, np, steps=5, warmup=3, autotune=True, count=512, wmin=10, wmax=22, dist=None):
     """512 hardware-efficient-ansatz circuits (width U{10..22}, depth U{4..12}
     layers of RY+RZ per qubit and a CNOT ring, observable sum_i Z_i): forward
     <O> and the full adjoint gradient of every circuit per run, one persistent
     kernel replayed as a CUDA graph.  Baseline: the parameter-shift rule with
     one kernel per gate (2 executes per parameterised occurrence), timed on a
-    width-stratified sample of the same circuits and summed over the batch."""
+    width-stratified sample of the same circuits and summed over the batch.
+    With dist (N ranks): each rank runs its balanced share of the circuits,
+    timings are the slowest rank's, results are gathered once; rank 0 returns
+    the report, the others None."""
     import torch
 
+    from quantumsimevo_b200 import distributed as D
     from quantumsimevo_b200.batch import Batch
     from quantumsimevo_b200.circuit import StateVector
     hb = W.hea_batch(count, wmin, wmax, 4, 12, seed=5)
     circs = [(w, ops, len(p), obs) for (w, ops, p, obs) in hb]
     params = np.concatenate([p for (_, _, p, _) in hb])
+    rank, world = (dist.get_rank(), dist.get_world_size()) if dist else (0, 1)
+    idx = D.shard_for_rank(circs, rank, world) if dist else list(range(len(circs)))
+    mine = [circs[i] for i in idx]
+    my_params = D.local_params(circs, params, idx)
+    local = dev.index
     t0 = time.perf_counter()
-    b = Batch(circs, dev)
+    b = Batch(mine, dev)
     cfg = None
     if autotune:
-        cache = os.path.join(tempfile.gettempdir(), "qse_batch_autotune.json")
-        b.run(params)
+        cache = os.path.join(tempfile.gettempdir(), f"qse_batch_autotune_r{rank}.json")
+        b.run(my_params)
         cfg = b.autotune(cache)
     t_setup = time.perf_counter() - t0
-    local = dev.index
-    p_t = torch.tensor(params, dtype=torch.float64, device=f"cuda:{local}")
-    v_t = torch.zeros(len(circs), dtype=torch.float64, device=f"cuda:{local}")
-    g_t = torch.zeros(params.size, dtype=torch.float64, device=f"cuda:{local}")
+    p_t = torch.tensor(my_params, dtype=torch.float64, device=f"cuda:{local}")
+    v_t = torch.zeros(len(mine), dtype=torch.float64, device=f"cuda:{local}")
+    g_t = torch.zeros(max(1, my_params.size), dtype=torch.float64, device=f"cuda:{local}")
     torch.cuda.synchronize()
     for _ in range(warmup):
         b.run_device(p_t.data_ptr(), v_t.data_ptr(), g_t.data_ptr())
     dev.synchronize()
+    if dist:
+        dist.barrier()
     ms = C.c_float()
     L.check(L.lib.qse_ctx_record(dev.handle, 8))
     for _ in range(steps):
@@ -516,12 +530,21 @@ def bench_batch(dev, L, W, np, steps=5, warmup=3, autotune=True, count=512, wmin
     L.check(L.lib.qse_ctx_record(dev.handle, 9))
     L.check(L.lib.qse_ctx_elapsed(dev.handle, 8, 9, C.byref(ms)))
     run_ms = ms.value / steps
+    if dist:
+        run_ms = D.max_over_ranks(run_ms, dist, device=f"cuda:{local}")
     st = b.stats()
     # end to end: host parameters in, host values + gradients out
+    if dist:
+        dist.barrier()
     t0 = time.perf_counter()
     for _ in range(steps):
-        vals, grads = b.run(params)
+        vals, grads = b.run(my_params)
     e2e_ms = (time.perf_counter() - t0) / steps * 1e3
+    if dist:
+        e2e_ms = D.max_over_ranks(e2e_ms, dist, device=f"cuda:{local}")
+        vals, grads = D.gather_results(circs, idx, vals, grads, dist)
+        if rank != 0:
+            return None
 
     # accuracy: the single-state adjoint path on a few circuits of the batch
     off = np.concatenate([[0], np.cumsum([c[2] for c in circs])])
@@ -591,6 +614,8 @@ def bench_batch(dev, L, W, np, steps=5, warmup=3, autotune=True, count=512, wmin
         "hbm_gbs_multi_tile": hbm_gbs,
         "hbm_frac_multi_tile": hbm_gbs / hbm_peak,
         "setup_s": t_setup,
+        "ranks": world,
+        "rank0_circuits": len(mine),
         "timing": "device: CUDA events on the library stream around `steps` graph replays (device params); "
                   "e2e: host wall clock of qse_batch_run (params H2D, values+grads D2H); plain param-shift: "
                   "host wall clock of plain-kernel execute+<O> per width, scaled by depth and occurrences",
