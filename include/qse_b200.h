@@ -150,6 +150,9 @@ QSE_API int qse_ctx_elapsed(qse_ctx* ctx, int slot_a, int slot_b, float* ms);
  * returns (and clears) the count and summed milliseconds. */
 QSE_API int qse_ctx_time_passes(qse_ctx* ctx, int enabled);
 QSE_API int qse_ctx_pass_times(qse_ctx* ctx, uint64_t* launches, double* total_ms);
+/* the same, one duration per launch in launch order (up to cap of them);
+ * *count receives the number recorded; the record is cleared */
+QSE_API int qse_ctx_pass_time_list(qse_ctx* ctx, double* ms, size_t cap, size_t* count);
 
 /* ---- state vector ---------------------------------------------------- */
 /* StateVector::StateVector (StateVector.cpp:14-32): 2^n amplitudes, |0..0>. Device-resident. */

@@ -100,6 +100,7 @@ _SIGS = {
     "qse_ctx_elapsed": ([_vp, C.c_int, C.c_int, C.POINTER(C.c_float)], C.c_int),
     "qse_ctx_time_passes": ([_vp, C.c_int], C.c_int),
     "qse_ctx_pass_times": ([_vp, _pu64, _pd], C.c_int),
+    "qse_ctx_pass_time_list": ([_vp, _pd, _sz, C.POINTER(_sz)], C.c_int),
     "qse_sample_device": ([_vp, _vp, _sz, _u64, _vp], C.c_int),
     "qse_state_create": ([_vp, _u32, C.POINTER(_vp)], C.c_int),
     "qse_state_destroy": ([_vp], C.c_int),

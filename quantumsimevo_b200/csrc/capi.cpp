@@ -260,6 +260,23 @@ int qse_ctx_pass_times(qse_ctx* ctx, uint64_t* launches, double* total_ms)
     QSE_GUARD_END
 }
 
+int qse_ctx_pass_time_list(qse_ctx* ctx, double* ms, size_t cap, size_t* count)
+{
+    QSE_GUARD_BEGIN
+    need(ctx && count && (cap == 0 || ms), QSE_ERR_INVALID, "null argument");
+    bind_device(ctx);
+    QSE_CUDA(cudaStreamSynchronize(ctx->stream));
+    const size_t n = ctx->pass_events_used / 2;
+    *count = n;
+    for (size_t i = 0; i < n && i < cap; ++i) {
+        float t = 0.f;
+        QSE_CUDA(cudaEventElapsedTime(&t, ctx->pass_events[2 * i], ctx->pass_events[2 * i + 1]));
+        ms[i] = t;
+    }
+    ctx->pass_events_used = 0;
+    QSE_GUARD_END
+}
+
 int qse_state_create(qse_ctx* ctx, uint32_t nqubits, qse_state** out)
 {
     QSE_GUARD_BEGIN
@@ -307,8 +324,9 @@ int qse_state_reset(qse_state* st)
     QSE_GUARD_BEGIN
     need(st != nullptr, QSE_ERR_INVALID, "null state");
     bind_device(st->ctx);
-    for (uint32_t q = 0; q < 64; ++q) st->perm[q] = q;
-    qse::launch_init_zero_state(st);
+    // |0..0> without writing 16 B per amplitude: the next fused execute's first
+    // pass generates it; any other reader writes it first (materialize)
+    qse::mark_zero(st);
     QSE_GUARD_END
 }
 
@@ -318,6 +336,7 @@ int qse_state_upload(qse_state* st, const double* host)
     need(st != nullptr && host != nullptr, QSE_ERR_INVALID, "null argument");
     bind_device(st->ctx);
     for (uint32_t q = 0; q < 64; ++q) st->perm[q] = q;
+    st->lazy_zero = false;
     st->touch();
     QSE_CUDA(cudaMemcpyAsync(st->amp, host, st->size() * 16, cudaMemcpyHostToDevice, st->ctx->stream));
     QSE_CUDA(cudaStreamSynchronize(st->ctx->stream));
@@ -347,6 +366,7 @@ int qse_state_device_ptr(qse_state* st, void** dptr)
 {
     QSE_GUARD_BEGIN
     need(st != nullptr && dptr != nullptr, QSE_ERR_INVALID, "null argument");
+    qse::materialize(st);
     *dptr = st->amp;
     QSE_GUARD_END
 }

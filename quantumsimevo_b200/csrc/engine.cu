@@ -180,7 +180,8 @@ struct PassRunner {
         for (const auto& p : pl.passes) kq.push_back(p.k);
         if (!ctx->jit) return;
         srcs.reserve(pl.passes.size());
-        for (const auto& p : pl.passes) srcs.push_back(jit::generate(p, ns));
+        for (size_t i = 0; i < pl.passes.size(); ++i)
+            srcs.push_back(jit::generate(pl.passes[i], ns, i == 0 && ns == 1 && s->lazy_zero));
         std::vector<const jit::Source*> ptrs;
         for (const auto& s2 : srcs) ptrs.push_back(&s2);
         ks = jit::get_kernels(ptrs);
@@ -269,6 +270,7 @@ void execute_program(qse_state* st, const qse_op* ops, size_t nops, const double
         run_noise(st, noise, ops, nops, inj, ninj, stats);
     }
     uint64_t passes = 0;
+    if (!ctx->fusion || st->n < 4 || !ctx->jit) materialize(st);  // only JIT passes start from a lazy |0..0>
     if (!ctx->fusion || st->n < 4) {
         for (const plan::Gate& g : gates) apply_plain(st, g);
         passes = gates.size();
@@ -282,6 +284,7 @@ void execute_program(qse_state* st, const qse_op* ops, size_t nops, const double
         Uploaded up = upload_plan(ctx, pl);
         PassRunner runner(st, pl, up, 1, 4);
         for (size_t i = 0; i < up.args.size(); ++i) runner.run(i, nullptr, nullptr);
+        if (!up.args.empty()) st->lazy_zero = false;  // the first pass wrote every amplitude
         for (uint32_t q = 0; q < st->n; ++q) st->perm[q] = pl.perm_final[q];
         passes = pl.passes.size();
     }
@@ -295,6 +298,7 @@ void execute_program(qse_state* st, const qse_op* ops, size_t nops, const double
 
 void apply_single(qse_state* st, const qse_op& op)
 {
+    materialize(st);
     plan::Gate g = to_gate(op, op.theta);
     check_qubits(g, st->n);
     st->touch();
@@ -303,6 +307,7 @@ void apply_single(qse_state* st, const qse_op& op)
 
 void canonicalize(qse_state* st)
 {
+    materialize(st);
     st->touch();
     // restore logical == physical with physical qubit swaps (each a half sweep)
     for (uint32_t q = 0; q < st->n; ++q) {
@@ -405,6 +410,7 @@ ObsDev upload_obs(qse_state* st, const qse_observable* obs, char* dbase, char* h
 
 double run_obs(qse_state* st, const qse_observable* obs, double2* lam)
 {
+    materialize(st);
     qse_ctx* ctx = st->ctx;
     if (obs->nterms > 4096) fail(QSE_ERR_SIZE, "observable has too many terms");
     const uint64_t size = st->size();

@@ -313,8 +313,21 @@ void launch_swap(qse_state* st, uint32_t q0, uint32_t q1)
     count_launch(st->ctx);
 }
 
+void mark_zero(qse_state* st)
+{
+    for (uint32_t q = 0; q < 64; ++q) st->perm[q] = q;
+    st->lazy_zero = true;
+    st->touch();
+}
+
+void materialize(qse_state* st)
+{
+    if (st->lazy_zero) launch_init_zero_state(st);
+}
+
 void launch_init_zero_state(qse_state* st)
 {
+    st->lazy_zero = false;
     st->touch();
     QSE_CUDA(cudaMemsetAsync(st->amp, 0, st->size() * 16, st->ctx->stream));
     k_set_first<<<1, 1, 0, st->ctx->stream>>>(reinterpret_cast<double2*>(st->amp));
@@ -332,6 +345,7 @@ void scale_state(qse_state* st, double s)
 
 void launch_pauli_frame(qse_state* st, const int32_t* d_counts)
 {
+    materialize(st);
     qse_ctx* ctx = st->ctx;
     ctx->scratch.reserve(64 * sizeof(uint32_t) + 2 * sizeof(uint64_t));
     uint64_t* d_masks = static_cast<uint64_t*>(ctx->scratch.ptr);
@@ -357,6 +371,7 @@ void launch_pauli_frame(qse_state* st, const int32_t* d_counts)
 // gathered chunk by chunk through device scratch.
 void download_range(qse_state* st, uint64_t first, uint64_t count, double* host)
 {
+    materialize(st);
     qse_ctx* ctx = st->ctx;
     if (count == 0) return;
     if (st->identity_perm()) {
@@ -389,6 +404,7 @@ void download_logical(qse_state* st, double* host) { download_range(st, 0, st->s
 
 void permute_to_logical(qse_state* st, double* dst_device)
 {
+    materialize(st);
     qse_ctx* ctx = st->ctx;
     ctx->scratch.reserve(64 * sizeof(uint32_t));
     uint32_t perm[64] = {0};

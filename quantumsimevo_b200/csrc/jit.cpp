@@ -92,7 +92,9 @@ struct Gen {
     int thr[16];
     int nthr;
 
-    Gen(const plan::PassProgram& p, int nstates) : P(p), ns(nstates)
+    bool zero_in = false;   // generate |0..0> instead of loading (ns == 1)
+
+    Gen(const plan::PassProgram& p, int nstates, bool zero_input) : P(p), ns(nstates), zero_in(zero_input && nstates == 1)
     {
         R = 1u << P.rb;
         T = 1u << (P.k - P.rb);
@@ -236,7 +238,10 @@ struct Gen {
         o << "  u64 gb = " << gbase_expr() << ";\n";
         for (int s = 0; s < ns; ++s) o << "  double2 a" << s << "[" << R << "];\n";
         for (uint32_t j = 0; j < R; ++j) {
-            o << "  a0[" << j << "] = psi[gb | " << hex(reg_off(j)) << "];";
+            if (zero_in)
+                o << "  a0[" << j << "] = make_double2((gb | " << hex(reg_off(j)) << ") == 0ull ? 1.0 : 0.0, 0.0);";
+            else
+                o << "  a0[" << j << "] = psi[gb | " << hex(reg_off(j)) << "];";
             if (ns == 2) o << " a1[" << j << "] = lam[gb | " << hex(reg_off(j)) << "];";
             o << "\n";
         }
@@ -435,9 +440,9 @@ bool available(std::string* why)
     return nv.ok;
 }
 
-Source generate(const plan::PassProgram& p, int nstates)
+Source generate(const plan::PassProgram& p, int nstates, bool zero_input)
 {
-    Gen g(p, nstates);
+    Gen g(p, nstates, zero_input);
     Source s;
     s.code = g.run();
     s.prm = std::move(g.prm);

@@ -96,6 +96,7 @@ __global__ void __launch_bounds__(kThreads) k_sum_noalloc(const double* __restri
 
 double expectation_noalloc(qse_state* st, const qse_observable* obs)
 {
+    materialize(st);
     qse_ctx* ctx = st->ctx;
     if (obs->nterms > kMaxTerms)
         fail(QSE_ERR_SIZE, "qse_expectation_noalloc: at most " + std::to_string(kMaxTerms) + " observable terms");

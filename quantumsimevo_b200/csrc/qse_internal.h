@@ -80,6 +80,9 @@ struct qse_state {
     double* aux = nullptr;       // second state (adjoint |lambda>), allocated on first use
     uint32_t perm[64];           // logical qubit -> physical bit
     uint64_t version = 0;        // bumped by every call that writes the amplitudes
+    bool lazy_zero = false;      // the state is |0..0> (identity qubit map) but the array has
+                                 // not been written: the next fused execute generates it in its
+                                 // first pass, every other reader calls materialize() first
     // exact cumulative probabilities (sample.cu), valid while cdf_version == version
     qse::DevBuf cdf;
     uint64_t cdf_version = ~uint64_t(0);
@@ -126,6 +129,8 @@ void launch_rz(qse_state* st, uint32_t q, double c0, double s0, double c1, doubl
 void launch_cnot(qse_state* st, uint32_t c, uint32_t t);
 void launch_swap(qse_state* st, uint32_t q0, uint32_t q1);
 void launch_init_zero_state(qse_state* st);
+void mark_zero(qse_state* st);       // reset without writing: lazy |0..0>
+void materialize(qse_state* st);     // write a lazy |0..0> into the array (no-op otherwise)
 void launch_pauli_frame(qse_state* st, const int32_t* d_counts);      // Noise::applyPauliNoise
 void permute_to_logical(qse_state* st, double* dst_device);           // gather into logical order
 void scale_state(qse_state* st, double s);

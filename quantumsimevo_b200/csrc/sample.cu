@@ -804,6 +804,7 @@ GatherPlan make_gather(const qse_state* st)
 // the amplitudes change (sample() followed by measure() builds it once).
 CdfView build_cdf(qse_state* st)
 {
+    materialize(st);
     qse_ctx* ctx = st->ctx;
     const uint64_t size = st->size();
     if (st->cdf_version == st->version)

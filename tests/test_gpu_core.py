@@ -94,6 +94,51 @@ def test_qft_20q(dev):
     assert stats.passes <= 4
 
 
+def test_reset_then_every_reader_sees_zero_state(dev):
+    """Reset records |0..0> without writing the array; the next fused execute
+    generates it in its first pass and every other reader writes it first."""
+    n = 13
+    ops = W.random_circuit(n, 120, 17)
+    want = O.run(n, ops)
+    zero = np.zeros(1 << n, dtype=np.complex128)
+    zero[0] = 1.0
+    st = StateVector(n, dev)
+
+    def dirty():
+        L.check(L.lib.qse_execute(st.handle, L.dptr(ops), len(ops), None, 0, None, None, 0, None))
+        L.check(L.lib.qse_state_reset(st.handle))
+
+    dirty()
+    assert np.array_equal(st.download(), zero)
+    dirty()
+    L.check(L.lib.qse_execute(st.handle, L.dptr(ops), len(ops), None, 0, None, None, 0, None))
+    assert np.max(np.abs(st.download() - want)) <= TOL
+    dirty()
+    L.check(L.lib.qse_apply_h(st.handle, 0))
+    h = zero.copy()
+    h[0] = h[1] = 1 / np.sqrt(2)
+    assert np.max(np.abs(st.download() - h)) <= TOL
+    dirty()
+    out = np.zeros(8, dtype=np.uint64)
+    L.check(L.lib.qse_sample(st.handle, np.linspace(0.01, 0.99, 8).ctypes.data_as(L._pd), 8, 0,
+                             out.ctypes.data_as(L._pu64)))
+    assert np.all(out == 0)
+    dirty()
+    obs, keep = L.observable([1, 2], [1.0, 0.5], 0.25)
+    v = C.c_double()
+    L.check(L.lib.qse_expectation(st.handle, C.byref(obs), C.byref(v)))
+    assert abs(v.value - 1.75) <= TOL
+    dirty()
+    dev.set_fusion(False)
+    L.check(L.lib.qse_execute(st.handle, L.dptr(ops), len(ops), None, 0, None, None, 0, None))
+    dev.set_fusion(True, 12, 0)
+    assert np.max(np.abs(st.download() - want)) <= TOL
+    dirty()
+    swaps = W.to_array([(L.SWAP, 0, 5, -1, 0, 0.0, 1.0, (0.0,) * 8)] * 3)
+    L.check(L.lib.qse_execute(st.handle, L.dptr(swaps), len(swaps), None, 0, None, None, 0, None))
+    assert np.array_equal(st.download(), zero)
+
+
 def test_execute_twice_and_swap_relabel(dev):
     # Circuit::execute does not clear its queue: a second execute applies it again
     n = 11
