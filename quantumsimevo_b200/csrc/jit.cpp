@@ -223,6 +223,25 @@ struct Gen {
         for (uint32_t q = 0; q < 64; ++q)
             if ((P.outer_mask >> q) & 1) o << " ob |= (c & 1ull) << " << q << "; c >>= 1;";
         o << " (void)c; }\n";
+        if (zero_in) {
+            // |0..0> input: only the tile holding index 0 has a nonzero amplitude;
+            // every gate is linear, so every other tile's output is zero
+            // zeros stored in tile-local order m = tid + j*T (the tile always holds
+            // physical qubits 0..2, so consecutive threads write consecutive amplitudes)
+            const uint32_t lt = uint32_t(__builtin_ctz(T));
+            o << "  if (ob != 0ull) {\n    const u64 gz = ob";
+            for (uint32_t b = 0; b < lt; ++b)
+                o << " | ((u64)((tid >> " << b << ") & 1u) << " << int(P.tile_phys[b]) << ")";
+            o << ";\n";
+            for (uint32_t j = 0; j < R; ++j) {
+                uint64_t cj = 0;
+                const uint64_t m = uint64_t(j) * T;
+                for (uint32_t b = lt; b < P.k; ++b)
+                    if ((m >> b) & 1) cj |= uint64_t(1) << P.tile_phys[b];
+                o << "    psi[gz | " << hex(cj) << "] = make_double2(0.0, 0.0);\n";
+            }
+            o << "    return;\n  }\n";
+        }
         // prologue: per-CTA diagonal group values
         if (ng) {
             o << "  for (u32 g = tid; g < " << ng << "u; g += " << T << "u) {\n"
