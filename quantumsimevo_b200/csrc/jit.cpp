@@ -93,6 +93,7 @@ struct Gen {
     int nthr;
 
     bool zero_in = false;   // generate |0..0> instead of loading (ns == 1)
+    bool xb_used = false;   // the exchange buffer holds data some thread may still read
 
     Gen(const plan::PassProgram& p, int nstates, bool zero_input) : P(p), ns(nstates), zero_in(zero_input && nstates == 1)
     {
@@ -377,7 +378,9 @@ struct Gen {
             o << "    const u32 sr = " << slot_expr(nl) << ";\n";
             for (int s = 0; s < ns; ++s) {
                 const char* A = s ? "a1" : "a0";
-                o << "    __syncthreads();\n";
+                // the first exchange of a pass follows the prologue's barrier: nobody reads xb yet
+                if (xb_used) o << "    __syncthreads();\n";
+                xb_used = true;
                 for (uint32_t j = 0; j < R; ++j) o << "    xb[sw ^ " << woff[j] << "u] = " << A << "[" << j << "];\n";
                 o << "    __syncthreads();\n";
                 for (uint32_t j = 0; j < R; ++j)
