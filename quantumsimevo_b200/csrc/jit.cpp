@@ -239,7 +239,7 @@ struct Gen {
                 const uint64_t m = uint64_t(j) * T;
                 for (uint32_t b = lt; b < P.k; ++b)
                     if ((m >> b) & 1) cj |= uint64_t(1) << P.tile_phys[b];
-                o << "    psi[gz | " << hex(cj) << "] = make_double2(0.0, 0.0);\n";
+                o << "    psi[gz + " << hex(cj) << "] = make_double2(0.0, 0.0);\n";
             }
             o << "    return;\n  }\n";
         }
@@ -253,7 +253,8 @@ struct Gen {
         }
         if (ns == 2 && nslots) o << "  for (u32 i = tid; i < " << nslots * NW << "u; i += " << T << "u) wp[i] = 0.0;\n";
         o << "  __syncthreads();\n";
-        // load
+        // load (gb holds only thread and outer bits, the offsets only register
+        // bits: gb + off == gb | off, and the constant folds into the address)
         set_layout(P.layouts[P.layout0]);
         o << "  u64 gb = " << gbase_expr() << ";\n";
         for (int s = 0; s < ns; ++s) o << "  double2 a" << s << "[" << R << "];\n";
@@ -261,8 +262,8 @@ struct Gen {
             if (zero_in)
                 o << "  a0[" << j << "] = make_double2((gb | " << hex(reg_off(j)) << ") == 0ull ? 1.0 : 0.0, 0.0);";
             else
-                o << "  a0[" << j << "] = psi[gb | " << hex(reg_off(j)) << "];";
-            if (ns == 2) o << " a1[" << j << "] = lam[gb | " << hex(reg_off(j)) << "];";
+                o << "  a0[" << j << "] = psi[gb + " << hex(reg_off(j)) << "];";
+            if (ns == 2) o << " a1[" << j << "] = lam[gb + " << hex(reg_off(j)) << "];";
             o << "\n";
         }
         emit_acc_decls();
@@ -271,8 +272,8 @@ struct Gen {
 
         // store
         for (uint32_t j = 0; j < R; ++j) {
-            o << "  psi[gb | " << hex(reg_off(j)) << "] = a0[" << j << "];";
-            if (ns == 2) o << " lam[gb | " << hex(reg_off(j)) << "] = a1[" << j << "];";
+            o << "  psi[gb + " << hex(reg_off(j)) << "] = a0[" << j << "];";
+            if (ns == 2) o << " lam[gb + " << hex(reg_off(j)) << "] = a1[" << j << "];";
             o << "\n";
         }
         if (ns == 2 && nslots) {
