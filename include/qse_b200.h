@@ -207,6 +207,14 @@ QSE_API int qse_execute(qse_state* st, const qse_op* ops, size_t nops,
                         const double* params, size_t nparams,
                         qse_noise* noise, const double* injected_uniforms, size_t n_uniforms,
                         qse_exec_stats* stats);
+/* Circuit::execute over a gate list that also holds mid-circuit QSE_GATE_MEASURE
+ * and QSE_GATE_RESET_QUBIT gates (GateType::MEASURE / RESET_QUBIT, Structurs.h:10,
+ * which the reference's execute loop does not run): the gates between two such
+ * gates run fused as in qse_execute; a MEASURE on `target` writes its outcome to
+ * results[control] (GateCommand::resultIdx, Structurs.h:18); RESET_QUBIT resets
+ * `target`.  uniforms: one draw per MEASURE / RESET_QUBIT gate, in program order. */
+QSE_API int qse_execute_mid(qse_state* st, const qse_op* ops, size_t nops, const double* params, size_t nparams,
+                            const double* uniforms, size_t n_uniforms, int32_t* results, size_t n_results);
 
 /* Planner introspection (no device work, no GPU needed): JSON description of
  * the passes Circuit::execute would launch for ops on an n-qubit state with
@@ -241,6 +249,15 @@ QSE_API int qse_sample_device(qse_state* st, const double* d_uniforms, size_t ns
                               uint64_t* d_out);
 /* measure(): outcome for uniform u, then collapse to |outcome> (amplitude 1, all others 0) */
 QSE_API int qse_measure(qse_state* st, double u, uint64_t* out_index);
+/* StateVector::measureQubit (StateVector.cpp:158-185): prob1 = sum of |a_i|^2 over
+ * the basis states with the qubit set; outcome = (u < prob1); amplitudes of the
+ * other outcome become 0 and the rest are divided by sqrt(its probability).
+ * u in [0,1) stands in for the reference's random_device draw.  prob1 may be NULL. */
+QSE_API int qse_measure_qubit(qse_state* st, uint32_t qubit, double u, int32_t* outcome, double* prob1);
+/* StateVector::resetQubit (StateVector.cpp:187-221): the same draw, then the
+ * outcome's amplitudes (renormalised) move to the qubit-0 half and the qubit is
+ * left in |0>.  outcome and prob1 may be NULL. */
+QSE_API int qse_reset_qubit(qse_state* st, uint32_t qubit, double u, int32_t* outcome, double* prob1);
 /* Diagnostics of the exact-CDF scan on the current state: out = {chunks composed
  * in parallel, chunks walked block by block, blocks folded element by element,
  * blocks}.  Rebuilds the cumulative array. */

@@ -303,6 +303,62 @@ uint64_t orc_measure(double* st, unsigned n, double u)
     return collapsed;
 }
 
+/* StateVector.cpp:158-185 with the draw injected: prob1 summed in index order
+ * (the reduction with one OpenMP thread), outcome = u < prob1, the other half
+ * zeroed and the kept half divided by sqrt(probability of the outcome). */
+static double prob_one(const double* st, unsigned n, unsigned q)
+{
+    size_t size = (size_t)1 << n, bit = (size_t)1 << q;
+    double p1 = 0.0;
+    for (size_t i = 0; i < size; ++i)
+        if (i & bit) p1 += cnorm(AMP(st, i));
+    return p1;
+}
+
+int orc_measure_qubit(double* st, unsigned n, unsigned q, double u, double* prob1)
+{
+    size_t size = (size_t)1 << n, bit = (size_t)1 << q;
+    double p1 = prob_one(st, n, q);
+    int outcome = (u < p1) ? 1 : 0;
+    double norm = outcome ? sqrt(p1) : sqrt(1.0 - p1);
+    for (size_t i = 0; i < size; ++i) {
+        int one = (i & bit) != 0;
+        if (one != outcome) {
+            st[2 * i] = 0.0;
+            st[2 * i + 1] = 0.0;
+        } else {
+            st[2 * i] /= norm;
+            st[2 * i + 1] /= norm;
+        }
+    }
+    if (prob1) *prob1 = p1;
+    return outcome;
+}
+
+/* StateVector.cpp:187-221: the same draw; the outcome's amplitudes move to the
+ * qubit-0 half, renormalised, and the qubit-1 half is zeroed. */
+int orc_reset_qubit(double* st, unsigned n, unsigned q, double u, double* prob1)
+{
+    size_t size = (size_t)1 << n, bit = (size_t)1 << q, lower = bit - 1;
+    double p1 = prob_one(st, n, q);
+    int outcome = (u < p1) ? 1 : 0;
+    double nf = sqrt(outcome ? p1 : 1.0 - p1);
+    for (size_t i = 0; i < size / 2; ++i) {
+        size_t i0 = ((i & ~lower) << 1) | (i & lower), i1 = i0 | bit;
+        if (outcome == 0) {
+            st[2 * i0] /= nf;
+            st[2 * i0 + 1] /= nf;
+        } else {
+            st[2 * i0] = st[2 * i1] / nf;
+            st[2 * i0 + 1] = st[2 * i1 + 1] / nf;
+        }
+        st[2 * i1] = 0.0;
+        st[2 * i1 + 1] = 0.0;
+    }
+    if (prob1) *prob1 = p1;
+    return outcome;
+}
+
 /* ---------------- mt19937 (Matsumoto & Nishimura 1998) ---------------- */
 void orc_mt_seed(orc_mt* g, uint32_t seed)
 {

@@ -30,6 +30,10 @@ void   orc_cdf(const double* st, unsigned n, double* cum);
 size_t orc_lower_bound(const double* cum, size_t size, double target);
 void   orc_sample(const double* st, unsigned n, const double* u, size_t nshots, uint64_t* out);
 uint64_t orc_measure(double* st, unsigned n, double u);
+/* StateVector::measureQubit / resetQubit (StateVector.cpp:158-221), draw injected;
+ * return the outcome, *prob1 = the probability of the qubit being 1 */
+int orc_measure_qubit(double* st, unsigned n, unsigned q, double u, double* prob1);
+int orc_reset_qubit(double* st, unsigned n, unsigned q, double u, double* prob1);
 
 /* mt19937 + libstdc++ generate_canonical<double,53> */
 typedef struct orc_mt { uint32_t mt[624]; int idx; } orc_mt;

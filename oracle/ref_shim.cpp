@@ -266,6 +266,16 @@ void ref_statevector_set(void* svp, const double* in)
 }
 
 uint64_t ref_statevector_measure(void* svp) { Quiet q(g_quiet); return static_cast<StateVector*>(svp)->measure(); }
+int ref_statevector_measure_qubit(void* svp, unsigned qubit)
+{
+    Quiet q(g_quiet);
+    return static_cast<StateVector*>(svp)->measureQubit(qubit);
+}
+void ref_statevector_reset_qubit(void* svp, unsigned qubit)
+{
+    Quiet q(true);
+    static_cast<StateVector*>(svp)->resetQubit(qubit);
+}
 
 void ref_statevector_sample(void* svp, int shots, uint64_t* out)
 {

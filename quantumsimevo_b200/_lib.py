@@ -133,6 +133,9 @@ _SIGS = {
     "qse_plan_describe": ([_u32, _vp, _sz, _pd, _sz, _u32, _u32, C.c_char_p, _sz, C.POINTER(_sz)], C.c_int),
     "qse_sample": ([_vp, _pd, _sz, _u64, _pu64], C.c_int),
     "qse_measure": ([_vp, _d, _pu64], C.c_int),
+    "qse_measure_qubit": ([_vp, _u32, _d, C.POINTER(_i32), _pd], C.c_int),
+    "qse_reset_qubit": ([_vp, _u32, _d, C.POINTER(_i32), _pd], C.c_int),
+    "qse_execute_mid": ([_vp, _vp, _sz, _pd, _sz, _pd, _sz, C.POINTER(_i32), _sz], C.c_int),
     "qse_total_probability": ([_vp, _pd], C.c_int),
     "qse_expectation": ([_vp, C.POINTER(QseObservable), _pd], C.c_int),
     "qse_adjoint": ([_vp, _vp, _sz, _pd, _sz, C.POINTER(QseObservable), _pd, _pd], C.c_int),

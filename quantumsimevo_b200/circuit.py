@@ -90,6 +90,19 @@ class StateVector:
         check(lib.qse_state_download_range(self.handle, int(first), int(count), L.dptr(out)))
         return out
 
+    def measure_qubit(self, qubit: int, u: float | None = None) -> int:
+        """StateVector::measureQubit (StateVector.cpp:158-185): collapse one qubit,
+        return 0 or 1.  u: the uniform draw (default: numpy's generator)."""
+        u = float(np.random.random()) if u is None else float(u)
+        o = L.C.c_int32()
+        check(lib.qse_measure_qubit(self.handle, int(qubit), u, L.C.byref(o), None))
+        return int(o.value)
+
+    def reset_qubit(self, qubit: int, u: float | None = None) -> None:
+        """StateVector::resetQubit (StateVector.cpp:187-221): measure, leave the qubit in |0>."""
+        u = float(np.random.random()) if u is None else float(u)
+        check(lib.qse_reset_qubit(self.handle, int(qubit), u, None, None))
+
     def qubit_map(self) -> list:
         m = (L.C.c_uint32 * self.num_qubits)()
         check(lib.qse_state_qubit_map(self.handle, m))

@@ -490,6 +490,42 @@ int qse_execute(qse_state* st, const qse_op* ops, size_t nops, const double* par
     QSE_GUARD_END
 }
 
+int qse_execute_mid(qse_state* st, const qse_op* ops, size_t nops, const double* params, size_t nparams,
+                    const double* uniforms, size_t n_uniforms, int32_t* results, size_t n_results)
+{
+    QSE_GUARD_BEGIN
+    need(st != nullptr, QSE_ERR_INVALID, "null state");
+    need(nops == 0 || ops != nullptr, QSE_ERR_INVALID, "null ops");
+    // validate the measurement layout before anything runs
+    size_t nmr = 0;
+    for (size_t i = 0; i < nops; ++i) {
+        const int t = ops[i].type;
+        if (t != QSE_GATE_MEASURE && t != QSE_GATE_RESET_QUBIT) continue;
+        need(ops[i].target < st->n, QSE_ERR_QUBIT, "measured qubit out of range");
+        if (t == QSE_GATE_MEASURE)
+            need(results != nullptr && ops[i].control < n_results, QSE_ERR_INVALID, "result index out of range");
+        ++nmr;
+    }
+    need(nmr <= n_uniforms && (nmr == 0 || uniforms != nullptr), QSE_ERR_INVALID,
+         "one uniform per MEASURE / RESET_QUBIT gate is needed");
+    for (size_t k = 0; k < nmr; ++k)
+        need(uniforms[k] >= 0.0 && uniforms[k] < 1.0, QSE_ERR_INVALID, "uniforms must lie in [0,1)");
+    bind_device(st->ctx);
+    size_t start = 0, k = 0;
+    for (size_t i = 0; i <= nops; ++i) {
+        const bool mr = i < nops && (ops[i].type == QSE_GATE_MEASURE || ops[i].type == QSE_GATE_RESET_QUBIT);
+        if (!mr && i < nops) continue;
+        if (i > start) qse::execute_program(st, ops + start, i - start, params, nparams, nullptr, nullptr, 0, nullptr);
+        if (mr) {
+            const bool reset = ops[i].type == QSE_GATE_RESET_QUBIT;
+            const int outcome = qse::measure_or_reset_qubit(st, ops[i].target, uniforms[k++], reset, nullptr);
+            if (!reset) results[ops[i].control] = outcome;
+        }
+        start = i + 1;
+    }
+    QSE_GUARD_END
+}
+
 int qse_plan_describe(uint32_t nqubits, const qse_op* ops, size_t nops, const double* params, size_t nparams,
                       uint32_t tile_qubits, uint32_t max_gates_per_pass, char* buf, size_t buflen, size_t* needed)
 {
@@ -603,6 +639,27 @@ int qse_measure(qse_state* st, double u, uint64_t* out_index)
     need(u >= 0.0 && u < 1.0, QSE_ERR_INVALID, "u must lie in [0,1)");
     bind_device(st->ctx);
     *out_index = qse::measure(st, u);
+    QSE_GUARD_END
+}
+
+int qse_measure_qubit(qse_state* st, uint32_t qubit, double u, int32_t* outcome, double* prob1)
+{
+    QSE_GUARD_BEGIN
+    need(st != nullptr && outcome != nullptr, QSE_ERR_INVALID, "null argument");
+    need(u >= 0.0 && u < 1.0, QSE_ERR_INVALID, "u must lie in [0,1)");
+    bind_device(st->ctx);
+    *outcome = qse::measure_or_reset_qubit(st, qubit, u, false, prob1);
+    QSE_GUARD_END
+}
+
+int qse_reset_qubit(qse_state* st, uint32_t qubit, double u, int32_t* outcome, double* prob1)
+{
+    QSE_GUARD_BEGIN
+    need(st != nullptr, QSE_ERR_INVALID, "null argument");
+    need(u >= 0.0 && u < 1.0, QSE_ERR_INVALID, "u must lie in [0,1)");
+    bind_device(st->ctx);
+    const int o = qse::measure_or_reset_qubit(st, qubit, u, true, prob1);
+    if (outcome) *outcome = o;
     QSE_GUARD_END
 }
 

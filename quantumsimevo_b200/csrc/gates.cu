@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 
 namespace qse {
 namespace {
@@ -172,6 +173,60 @@ __global__ void __launch_bounds__(kBlock) k_swap(double2* __restrict__ a, uint64
 
 __global__ void k_set_first(double2* a) { a[0] = make_double2(1.0, 0.0); }
 
+// index of the j-th amplitude with physical bit b equal to v (j < 2^(n-1))
+__device__ __forceinline__ uint64_t with_bit(uint64_t j, uint32_t b, uint64_t v)
+{
+    const uint64_t lo = j & ((uint64_t(1) << b) - 1);
+    return ((j >> b) << (b + 1)) | (v << b) | lo;
+}
+
+// partial[block] = sum of |a_i|^2 (std::norm's two roundings, no FMA) over the
+// amplitudes with bit b set; grid-stride per thread, then a fixed-order tree
+__global__ void __launch_bounds__(kBlock) k_prob_bit(const double2* __restrict__ a, uint64_t half, uint32_t b,
+                                                     double* __restrict__ partial)
+{
+    __shared__ double sh[kBlock / 32];
+    double s = 0.0;
+    for (uint64_t j = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; j < half; j += uint64_t(gridDim.x) * blockDim.x) {
+        const double2 v = a[with_bit(j, b, 1)];
+        s += __dadd_rn(__dmul_rn(v.x, v.x), __dmul_rn(v.y, v.y));
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < kBlock / 32; ++w) t += sh[w];
+        partial[blockIdx.x] = t;
+    }
+}
+
+// StateVector::measureQubit's collapse (StateVector.cpp:173-182): amplitudes whose
+// bit differs from the outcome become 0, the others are divided by norm
+__global__ void __launch_bounds__(kBlock) k_collapse_bit(double2* __restrict__ a, uint64_t half, uint32_t b,
+                                                         uint64_t outcome, double norm)
+{
+    for (uint64_t j = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; j < half; j += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t keep = with_bit(j, b, outcome), drop = with_bit(j, b, outcome ^ 1);
+        const double2 v = a[keep];
+        a[keep] = make_double2(v.x / norm, v.y / norm);
+        a[drop] = make_double2(0.0, 0.0);
+    }
+}
+
+// StateVector::resetQubit's move (StateVector.cpp:203-215): the outcome's
+// amplitudes, divided by nf, land on the bit-0 half; the bit-1 half becomes 0
+__global__ void __launch_bounds__(kBlock) k_reset_bit(double2* __restrict__ a, uint64_t half, uint32_t b,
+                                                      uint64_t outcome, double nf)
+{
+    for (uint64_t j = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; j < half; j += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t i0 = with_bit(j, b, 0), i1 = with_bit(j, b, 1);
+        const double2 v = a[outcome ? i1 : i0];
+        a[i0] = make_double2(v.x / nf, v.y / nf);
+        a[i1] = make_double2(0.0, 0.0);
+    }
+}
+
 __global__ void __launch_bounds__(kBlock) k_scale(double2* __restrict__ a, uint64_t count, double s)
 {
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < count;
@@ -323,6 +378,44 @@ void mark_zero(qse_state* st)
 void materialize(qse_state* st)
 {
     if (st->lazy_zero) launch_init_zero_state(st);
+}
+
+// StateVector::measureQubit / resetQubit (StateVector.cpp:158-221) with the
+// draw u injected: prob1 = sum of |a_i|^2 over the qubit's 1 half (fixed-order
+// reduction), outcome = u < prob1, then the collapse (or the reset move).
+int measure_or_reset_qubit(qse_state* st, uint32_t q, double u, bool reset, double* prob1)
+{
+    if (q >= st->n) fail(QSE_ERR_QUBIT, "qubit index out of range");
+    materialize(st);
+    qse_ctx* ctx = st->ctx;
+    const uint32_t b = st->perm[q];
+    const uint64_t half = st->size() / 2;
+    const unsigned grid = unsigned(std::min<uint64_t>((half + kBlock - 1) / kBlock, uint64_t(ctx->num_sms) * 8));
+    ctx->scratch.reserve(size_t(grid) * 8 + 16);
+    ctx->host_small.reserve(size_t(grid) * 8 + 16);
+    QSE_CUDA(cudaStreamSynchronize(ctx->stream));  // host_small may still feed an earlier copy
+    double* part = static_cast<double*>(ctx->scratch.ptr);
+    k_prob_bit<<<grid, kBlock, 0, ctx->stream>>>(reinterpret_cast<const double2*>(st->amp), half, b, part);
+    QSE_CUDA(cudaGetLastError());
+    count_launch(ctx);
+    double* hp = static_cast<double*>(ctx->host_small.ptr);
+    QSE_CUDA(cudaMemcpyAsync(hp, part, size_t(grid) * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    QSE_CUDA(cudaStreamSynchronize(ctx->stream));
+    double p1 = 0.0;
+    for (unsigned i = 0; i < grid; ++i) p1 += hp[i];
+    const int outcome = (u < p1) ? 1 : 0;
+    const double norm = std::sqrt(outcome ? p1 : 1.0 - p1);
+    st->touch();
+    if (reset)
+        k_reset_bit<<<grid, kBlock, 0, ctx->stream>>>(reinterpret_cast<double2*>(st->amp), half, b, uint64_t(outcome),
+                                                      norm);
+    else
+        k_collapse_bit<<<grid, kBlock, 0, ctx->stream>>>(reinterpret_cast<double2*>(st->amp), half, b,
+                                                         uint64_t(outcome), norm);
+    QSE_CUDA(cudaGetLastError());
+    count_launch(ctx);
+    if (prob1) *prob1 = p1;
+    return outcome;
 }
 
 void launch_init_zero_state(qse_state* st)

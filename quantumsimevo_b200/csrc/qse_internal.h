@@ -130,6 +130,8 @@ void launch_cnot(qse_state* st, uint32_t c, uint32_t t);
 void launch_swap(qse_state* st, uint32_t q0, uint32_t q1);
 void launch_init_zero_state(qse_state* st);
 void mark_zero(qse_state* st);       // reset without writing: lazy |0..0>
+// StateVector::measureQubit (reset = false) / resetQubit (reset = true), draw u injected
+int measure_or_reset_qubit(qse_state* st, uint32_t qubit, double u, bool reset, double* prob1);
 void materialize(qse_state* st);     // write a lazy |0..0> into the array (no-op otherwise)
 void launch_pauli_frame(qse_state* st, const int32_t* d_counts);      // Noise::applyPauliNoise
 void permute_to_logical(qse_state* st, double* dst_device);           // gather into logical order

@@ -39,6 +39,8 @@ def _load_oracle():
         "orc_philox_uniform_pair": ([_u64, _u64, _pd, _pd], None),
         "orc_noise_init": ([C.POINTER(OrcNoise), C.c_uint, C.POINTER(QseNoiseConfig)], None),
         "orc_noise_accumulate": ([C.POINTER(OrcNoise), C.c_int, C.c_uint, _pd], C.c_int),
+        "orc_measure_qubit": ([_vp, C.c_uint, C.c_uint, C.c_double, _pd], C.c_int),
+        "orc_reset_qubit": ([_vp, C.c_uint, C.c_uint, C.c_double, _pd], C.c_int),
         "orc_execute": ([_vp, C.c_uint, _vp, _sz, _pd, C.POINTER(OrcNoise), _pd, _sz], C.c_int),
         "orc_expectation": ([_vp, C.c_uint, C.POINTER(QseObservable)], _d),
         "orc_adjoint": ([C.c_uint, _vp, _sz, _pd, _sz, C.POINTER(QseObservable), _pd], _d),
@@ -153,6 +155,19 @@ def noise_decisions(n, ops, cfg):
     return list(nz.bit[:n]), list(nz.phase[:n])
 
 
+def measure_qubit(st, n, q, u):
+    """StateVector::measureQubit with the draw u; returns (outcome, prob1), st collapsed in place."""
+    p = C.c_double()
+    o = oracle.orc_measure_qubit(st.ctypes.data_as(_vp), n, q, u, C.byref(p))
+    return o, p.value
+
+
+def reset_qubit(st, n, q, u):
+    p = C.c_double()
+    o = oracle.orc_reset_qubit(st.ctypes.data_as(_vp), n, q, u, C.byref(p))
+    return o, p.value
+
+
 def philox_pair(seed, counter):
     a, b = C.c_double(), C.c_double()
     oracle.orc_philox_uniform_pair(seed, counter, C.byref(a), C.byref(b))
@@ -190,6 +205,8 @@ def load_reference(gpu=False):
         "ref_backend_mark_host_dirty": ([_vp], None),
         "ref_statevector_get": ([_vp, _vp], None),
         "ref_statevector_set": ([_vp, _vp], None),
+        "ref_statevector_measure_qubit": ([_vp, C.c_uint], C.c_int),
+        "ref_statevector_reset_qubit": ([_vp, C.c_uint], None),
     }
     for name, (a, r) in sigs.items():
         f = getattr(lib, name)

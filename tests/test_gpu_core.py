@@ -381,3 +381,59 @@ def test_adjoint_every_parameterised_type(dev):
     vw, gw = O.adjoint(n, ops, params, obs)
     assert abs(v - vw) <= 1e-10
     assert np.max(np.abs(g - gw)) <= 1e-10
+
+
+# ---------------------------------------------------------------- mid-circuit measurement
+@pytest.mark.parametrize("n", [5, 12, 17])
+def test_measure_and_reset_qubit_match_oracle(dev, n):
+    rng = np.random.default_rng(n)
+    for rep in range(4):
+        ops = W.random_circuit(n, 20 * n, 6000 + 10 * n + rep)  # SWAPs relabel the qubit map
+        want = O.run(n, ops)
+        q = int(rng.integers(0, n))
+        u = float(rng.random())
+        for which in ("measure", "reset"):
+            st = StateVector(n, dev)
+            L.check(L.lib.qse_execute(st.handle, L.dptr(ops), len(ops), None, 0, None, None, 0, None))
+            o = C.c_int32()
+            p1 = C.c_double()
+            fn = L.lib.qse_measure_qubit if which == "measure" else L.lib.qse_reset_qubit
+            L.check(fn(st.handle, q, u, C.byref(o), C.byref(p1)))
+            ref = want.copy()
+            ro, rp1 = (O.measure_qubit if which == "measure" else O.reset_qubit)(ref, n, q, u)
+            assert abs(p1.value - rp1) <= 1e-12
+            if abs(u - rp1) > 1e-9:
+                assert o.value == ro
+                assert np.max(np.abs(st.download() - ref)) <= TOL
+
+
+def test_execute_mid_circuit_measure_and_reset(dev):
+    n = 11
+    rng = np.random.default_rng(3)
+    parts = [W.random_circuit(n, 60, 6100 + k) for k in range(4)]
+    # MEASURE: target = qubit, control = result index (GateCommand::resultIdx)
+    mid = [W.to_array([(L.MEASURE, 3, 1, -1, 0, 0.0, 1.0, (0.0,) * 8)]),
+           W.to_array([(L.RESET_QUBIT, 7, 0, -1, 0, 0.0, 1.0, (0.0,) * 8)]),
+           W.to_array([(L.MEASURE, 0, 0, -1, 0, 0.0, 1.0, (0.0,) * 8)])]
+    ops = np.concatenate([parts[0], mid[0], parts[1], mid[1], parts[2], mid[2], parts[3]])
+    u = rng.random(3)
+    st = StateVector(n, dev)
+    res = np.full(2, -1, dtype=np.int32)
+    L.check(L.lib.qse_execute_mid(st.handle, L.dptr(ops), len(ops), None, 0, u.ctypes.data_as(L._pd), 3,
+                                  res.ctypes.data_as(C.POINTER(C.c_int32)), 2))
+    ref = O.run(n, parts[0])
+    r1, _ = O.measure_qubit(ref, n, 3, u[0])
+    ref = O.run_on(ref, n, parts[1])
+    O.reset_qubit(ref, n, 7, u[1])
+    ref = O.run_on(ref, n, parts[2])
+    r0, _ = O.measure_qubit(ref, n, 0, u[2])
+    ref = O.run_on(ref, n, parts[3])
+    assert list(res) == [r0, r1]
+    assert np.max(np.abs(st.download() - ref)) <= TOL
+    # too few draws / a result index outside the array are rejected before anything runs
+    with pytest.raises(L.QseError):
+        L.check(L.lib.qse_execute_mid(st.handle, L.dptr(ops), len(ops), None, 0, u.ctypes.data_as(L._pd), 2,
+                                      res.ctypes.data_as(C.POINTER(C.c_int32)), 2))
+    with pytest.raises(L.QseError):
+        L.check(L.lib.qse_execute_mid(st.handle, L.dptr(ops), len(ops), None, 0, u.ctypes.data_as(L._pd), 3,
+                                      res.ctypes.data_as(C.POINTER(C.c_int32)), 1))

@@ -95,3 +95,41 @@ def test_reference_sample_matches_lower_bound_semantics(ref):
     ref.ref_circuit_free(h)
     p = np.abs(st) ** 2
     assert np.all(p[out.astype(np.int64)] > 0)
+
+
+@pytest.mark.parametrize("which", ["measure", "reset"])
+def test_measure_reset_qubit_oracle_matches_reference(ref, which):
+    """StateVector::measureQubit / resetQubit draw from random_device, so the
+    reference picks the outcome; the oracle, given a draw that forces the same
+    outcome (u = 0 gives 1 whenever prob1 > 0, u close to 1 gives 0), must leave
+    the same state.  prob1's summation order differs (OpenMP), hence 1e-12."""
+    n = 7
+    for rep in range(12):
+        ops = W.random_circuit(n, 60, 3100 + rep, with_2x2=False)
+        st = O.run(n, ops)
+        q = rep % n
+        sv = ref.ref_statevector_new(n)
+        ref.ref_statevector_set(sv, np.ascontiguousarray(st).ctypes.data_as(C.c_void_p))
+        if which == "measure":
+            outcome = ref.ref_statevector_measure_qubit(sv, q)
+        else:
+            before = st.copy()
+            ref.ref_statevector_reset_qubit(sv, q)
+        got = np.empty_like(st)
+        ref.ref_statevector_get(sv, got.ctypes.data_as(C.c_void_p))
+        ref.ref_statevector_free(sv)
+        mine = st.copy()
+        if which == "measure":
+            o, p1 = O.measure_qubit(mine, n, q, 0.0 if outcome == 1 else 1.0 - 1e-15)
+            assert o == outcome
+        else:
+            # the reference does not report its outcome: both must match one of the two
+            a, b = before.copy(), before.copy()
+            O.reset_qubit(a, n, q, 0.0)
+            O.reset_qubit(b, n, q, 1.0 - 1e-15)
+            mine = a if np.max(np.abs(got - a)) < np.max(np.abs(got - b)) else b
+        assert np.max(np.abs(got - mine)) <= 1e-12
+        idx = np.arange(1 << n)
+        if which == "reset":
+            assert np.all(mine[(idx >> q) & 1 == 1] == 0)
+        assert abs(np.sum(np.abs(mine) ** 2) - 1.0) < 1e-12
