@@ -190,29 +190,38 @@ class Circuit:
     def pauli_z(self, q):
         self._push(L.make_op(L.Z, self._q(q)), f"PauliZ on qubit {q}")
 
-    def phase(self, theta, q):
-        self._push(L.make_op(L.PHASE, self._q(q), theta=float(theta)), f"Phase shift on qubit {q}")
+    # Parameterised angles (no counterpart in the reference's pybind module,
+    # QuantumSimEvoPy.cpp:11-40): with param=k the gate's angle is
+    # theta + coeff * params[k], params given to execute() / gradient().
+    def phase(self, theta, q, param: int = -1, coeff: float = 1.0):
+        self._push(L.make_op(L.PHASE, self._q(q), theta=float(theta), param=int(param), coeff=float(coeff)),
+                   f"Phase shift on qubit {q}")
 
-    def rotate_x(self, theta, q):
-        self._push(L.make_op(L.RX, self._q(q), theta=float(theta)), f"RX on qubit {q}")
+    def rotate_x(self, theta, q, param: int = -1, coeff: float = 1.0):
+        self._push(L.make_op(L.RX, self._q(q), theta=float(theta), param=int(param), coeff=float(coeff)),
+                   f"RX on qubit {q}")
 
-    def rotate_y(self, theta, q):
-        self._push(L.make_op(L.RY, self._q(q), theta=float(theta)), f"RY on qubit {q}")
+    def rotate_y(self, theta, q, param: int = -1, coeff: float = 1.0):
+        self._push(L.make_op(L.RY, self._q(q), theta=float(theta), param=int(param), coeff=float(coeff)),
+                   f"RY on qubit {q}")
 
-    def rotate_z(self, theta, q):
-        self._push(L.make_op(L.RZ, self._q(q), theta=float(theta)), f"RZ on qubit {q}")
+    def rotate_z(self, theta, q, param: int = -1, coeff: float = 1.0):
+        self._push(L.make_op(L.RZ, self._q(q), theta=float(theta), param=int(param), coeff=float(coeff)),
+                   f"RZ on qubit {q}")
 
     def cnot(self, control, target):
         self._push(L.make_op(L.CNOT, self._q(target), self._q(control)),
                    f"CNOT (control: {control}, target: {target})")
 
-    def cphase(self, theta, control, target):
-        self._push(L.make_op(L.CPHASE, self._q(target), self._q(control), float(theta)),
+    def cphase(self, theta, control, target, param: int = -1, coeff: float = 1.0):
+        self._push(L.make_op(L.CPHASE, self._q(target), self._q(control), float(theta), param=int(param),
+                             coeff=float(coeff)),
                    f"CPhase (theta: {theta}, control: {control}, target: {target})")
 
-    def mcphase(self, theta, controls, target):
+    def mcphase(self, theta, controls, target, param: int = -1, coeff: float = 1.0):
         ctl = [self._q(c) for c in controls]
-        self._push(L.make_op(L.MCPHASE, self._q(target), 0, float(theta), controls=ctl),
+        self._push(L.make_op(L.MCPHASE, self._q(target), 0, float(theta), controls=ctl, param=int(param),
+                             coeff=float(coeff)),
                    f"MCPhase (theta: {theta}, target: {target}, controls: {' '.join(map(str, ctl))})")
 
     def swap(self, q0, q1):
@@ -230,10 +239,11 @@ class Circuit:
         return L.as_ops(self._ops)
 
     # ---- execution & measurement ----
-    def execute(self, print_steps: bool = False, noise_uniforms=None):
+    def execute(self, print_steps: bool = False, noise_uniforms=None, params=None):
         """Replay the queue (Circuit.cpp:64-120).  With noise, the draws for each
         gate in the rate map come from the noise RNG, or from ``noise_uniforms``
-        (two per noisy gate) when the noise RNG is ``RNG_INJECTED``."""
+        (two per noisy gate) when the noise RNG is ``RNG_INJECTED``.  params:
+        values of the parameters that queued gates reference (param=k)."""
         if print_steps:
             print("Initial state: |0...0>")
             for d in self._desc:
@@ -246,7 +256,9 @@ class Circuit:
             inj = np.ascontiguousarray(np.asarray(noise_uniforms, dtype=np.float64))
             ninj = inj.size
         t0 = time.perf_counter()
-        check(lib.qse_execute(self.state.handle, L.dptr(ops) if len(ops) else None, len(ops), None, 0,
+        p = None if params is None else np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(-1))
+        check(lib.qse_execute(self.state.handle, L.dptr(ops) if len(ops) else None, len(ops),
+                              p.ctypes.data_as(L._pd) if p is not None else None, 0 if p is None else p.size,
                               self.noise.handle if self.noise else None,
                               inj.ctypes.data_as(L._pd) if inj is not None else None, ninj, L.C.byref(stats)))
         self.last_stats = stats
@@ -298,6 +310,37 @@ class Circuit:
             self.noise.reset_stats()
         self._ops.clear()
         self._desc.clear()
+
+    def measure_qubit(self, q, uniform=None) -> int:
+        """StateVector::measureQubit: collapse one qubit, return 0 or 1."""
+        return self.state.measure_qubit(self._q(q), uniform)
+
+    def reset_qubit(self, q, uniform=None) -> None:
+        """StateVector::resetQubit: measure one qubit and leave it in |0>."""
+        self.state.reset_qubit(self._q(q), uniform)
+
+    # ---- observables and gradients (no counterpart in the reference) ----
+    def expectation(self, zmasks, weights, constant: float = 0.0) -> float:
+        """<psi|O|psi> of the current state for O = constant + sum_t weights[t] Z-string(zmasks[t])
+        (zmask bit q = a Z on qubit q)."""
+        obs, keep = L.observable(zmasks, weights, constant)
+        v = L.C.c_double()
+        check(lib.qse_expectation(self.state.handle, L.C.byref(obs), L.C.byref(v)))
+        return v.value
+
+    def gradient(self, params, zmasks, weights, constant: float = 0.0):
+        """Runs the queued gates from |0..0> with ``params`` and returns
+        (<O>, d<O>/d params) by the adjoint sweep (one forward and one reverse
+        sweep over the state, whatever the number of parameters)."""
+        p = np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(-1))
+        obs, keep = L.observable(zmasks, weights, constant)
+        ops = self.ops
+        v = L.C.c_double()
+        g = np.zeros(max(1, p.size))
+        check(lib.qse_adjoint(self.state.handle, L.dptr(ops) if len(ops) else None, len(ops),
+                              p.ctypes.data_as(L._pd), p.size, L.C.byref(obs), L.C.byref(v),
+                              g.ctypes.data_as(L._pd)))
+        return v.value, g[: p.size]
 
     # ---- utilities ----
     def get_state_vector(self) -> np.ndarray:

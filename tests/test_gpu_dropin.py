@@ -111,3 +111,44 @@ def test_torch_autograd_matches_oracle_and_fd():
     with torch.no_grad():
         v2 = pc.expectation(torch.tensor(params))
     assert abs(v2.item() - vw) <= 1e-10
+
+
+def test_python_circuit_parameters_expectation_gradient_measure_qubit():
+    """The Python surface beyond the reference's pybind module: parameterised
+    gates, execute(params), expectation, gradient (adjoint) and measure_qubit,
+    each against the oracle."""
+    import numpy as np
+
+    import oracle_ffi as O
+    from quantumsimevo_b200 import _lib as L
+    from quantumsimevo_b200.circuit import Circuit
+    n = 9
+    c = Circuit(n, seed=1)
+    for q in range(n):
+        c.hadamard(q)
+    for layer in range(2):
+        for q in range(n - 1):
+            c.cphase(0.0, q, q + 1, param=layer, coeff=-2.0)
+        for q in range(n):
+            c.rotate_x(0.1, q, param=2 + layer, coeff=2.0)
+        c.rotate_z(0.3, layer, param=4)
+        c.mcphase(0.2, [0, 1], 5, param=4, coeff=0.5)
+    params = np.array([0.3, 1.1, 0.7, 0.2, 0.9])
+    zm, wt, const = [1 << q for q in range(n)] + [0b11], [0.5] * n + [-1.0], 0.25
+    c.execute(params=params)
+    want = O.run(n, c.ops, params)
+    assert np.max(np.abs(c.get_state_vector() - want)) <= 1e-12
+    obs, keep = L.observable(zm, wt, const)
+    assert abs(c.expectation(zm, wt, const) - O.expectation(want, n, obs)) <= 1e-12
+    v, g = c.gradient(params, zm, wt, const)
+    vw, gw = O.adjoint(n, c.ops, params, obs)
+    assert abs(v - vw) <= 1e-10 and np.max(np.abs(g - gw)) <= 1e-10
+    c.reset()
+    c.hadamard(2)
+    c.cnot(2, 6)
+    c.execute()
+    o = c.measure_qubit(6, uniform=0.25)
+    st = c.get_state_vector()
+    assert o in (0, 1)
+    idx = 1 << 2 | 1 << 6 if o else 0
+    assert abs(abs(st[idx]) - 1.0) <= 1e-12
