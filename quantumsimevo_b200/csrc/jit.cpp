@@ -206,19 +206,210 @@ struct Gen {
         for (uint32_t i = P.rb; i < 4; ++i) o << "  " << ty << " ar" << i << " = " << one << "; (void)ar" << i << ";\n";
     }
 
+    // ---- acc_mul: merged diagonal runs ----
+    // Diagonal ops between two non-diagonal ones commute.  Each run becomes
+    // one factor per register mask M (the product of its K_PHD groups, its
+    // flushed accumulator chain, or, for M = 0, the K_ACC_THR chain times the
+    // pass constant); the registers then take the products of the factors
+    // whose masks they contain, built through a prefix trie when that needs
+    // fewer complex multiplies than one multiply per (factor, register).
+    // Factors with two or more lane-conditioned groups read a per-CTA table
+    // over the 32 lanes, built once in the prologue; groups conditioned on
+    // warp bits stay per-thread multiplies (uniform within a warp).
+    struct Item { uint16_t tcond; uint16_t g; };
+    struct Fac { std::vector<Item> items; bool hc = false; double ca = 1.0, cb = 0.0; };
+    static constexpr uint32_t kMaxTables = 32;
+    std::vector<plan::KOp> run_ops;
+    std::vector<Item> chain[5];   // pending accumulator groups: ar0..ar3, at
+    std::ostringstream tabs;      // prologue code building the lane tables
+    uint32_t ntab = 0;
+    uint32_t nvar = 0;
+
+    static bool diag_kind(uint8_t k)
+    {
+        using namespace plan;
+        return k == K_ACC_THR || k == K_ACC_REG || k == K_PHD || k == K_FLUSH_REG || k == K_FLUSH_ALL;
+    }
+
+    void emit_op(const plan::KOp& op)
+    {
+        if (P.acc_mul) {
+            if (diag_kind(op.kind)) { run_ops.push_back(op); return; }
+            flush_run();
+        }
+        emit(op);
+    }
+
+    static std::string cond_t(const char* v, uint16_t tc)
+    {
+        return std::string("((") + v + " & " + std::to_string(tc) + "u) == " + std::to_string(tc) + "u)";
+    }
+
+    std::string emit_factor(const Fac& F)
+    {
+        std::vector<Item> L, W;
+        for (const Item& it : F.items) ((it.tcond & ~31u) == 0 ? L : W).push_back(it);
+        const std::string v = "f" + std::to_string(nvar++);
+        std::string cst;
+        if (F.hc) {
+            const uint32_t ci = push(F.ca);
+            push(F.cb);
+            cst = "make_double2(P.v[" + std::to_string(ci) + "], P.v[" + std::to_string(ci + 1) + "])";
+        }
+        if (ntab < kMaxTables && (L.size() >= 2 || (L.size() == 1 && F.hc))) {
+            const uint32_t t = ntab++;
+            tabs << "  if ((tid >> 5) == " << (t % NW) << "u) { const u32 l = tid & 31u; double2 v = "
+                 << (F.hc ? cst : std::string("make_double2(1.0, 0.0)")) << ";";
+            for (const Item& it : L) {
+                if (it.tcond) tabs << " if (" << cond_t("l", it.tcond) << ")";
+                tabs << " v = cmul(v, gv[" << it.g << "]);";
+            }
+            tabs << " tb[" << t * 32 << "u + l] = v; }\n";
+            o << "    double2 " << v << " = tb[" << t * 32 << "u + (tid & 31u)];\n";
+        } else {
+            size_t i = 0;
+            o << "    double2 " << v << " = ";
+            if (F.hc) o << cst;
+            else if (!L.empty()) {
+                const Item& it = L[i++];
+                if (it.tcond) o << cond_t("tid", it.tcond) << " ? gv[" << it.g << "] : make_double2(1.0, 0.0)";
+                else o << "gv[" << it.g << "]";
+            } else o << "make_double2(1.0, 0.0)";
+            o << ";\n";
+            for (; i < L.size(); ++i) {
+                o << "    ";
+                if (L[i].tcond) o << "if (" << cond_t("tid", L[i].tcond) << ") ";
+                o << v << " = cmul(" << v << ", gv[" << L[i].g << "]);\n";
+            }
+        }
+        for (const Item& it : W)
+            o << "    if (" << cond_t("tid", it.tcond) << ") " << v << " = cmul(" << v << ", gv[" << it.g << "]);\n";
+        return v;
+    }
+
+    void flush_run()
+    {
+        using namespace plan;
+        if (run_ops.empty()) return;
+        std::map<int, Fac> fac;
+        auto take = [&](int c, int mask) {
+            std::vector<Item>& d = fac[mask].items;
+            d.insert(d.end(), chain[c].begin(), chain[c].end());
+            chain[c].clear();
+        };
+        for (const KOp& op : run_ops) {
+            switch (op.kind) {
+            case K_ACC_REG: chain[op.p].push_back(Item{op.tcond, op.g}); break;
+            case K_ACC_THR: chain[4].push_back(Item{op.tcond, op.g}); break;
+            case K_PHD: fac[op.f].items.push_back(Item{op.tcond, op.g}); break;
+            case K_FLUSH_REG: take(op.p, 1 << op.p); break;
+            case K_FLUSH_ALL: {
+                for (uint32_t r = 0; r < P.rb; ++r)
+                    if ((op.f >> r) & 1) take(int(r), 1 << r);
+                take(4, 0);
+                if (!(op.a == 1.0 && op.b == 0.0)) {
+                    Fac& f = fac[0];
+                    const double a = f.ca * op.a - f.cb * op.b, b = f.ca * op.b + f.cb * op.a;
+                    f.ca = a;
+                    f.cb = b;
+                    f.hc = true;
+                }
+                break;
+            }
+            default: break;
+            }
+        }
+        run_ops.clear();
+        for (auto it = fac.begin(); it != fac.end();)
+            it = (it->second.items.empty() && !it->second.hc) ? fac.erase(it) : std::next(it);
+        if (fac.empty()) return;
+        o << "  {\n";
+        std::vector<int> masks;
+        std::map<int, std::string> val;
+        for (auto& kv : fac) {
+            masks.push_back(kv.first);
+            val[kv.first] = emit_factor(kv.second);
+        }
+        std::stable_sort(masks.begin(), masks.end(),
+                         [](int a, int b) { return __builtin_popcount(a) < __builtin_popcount(b); });
+        // per register: the masks it contains, in the sorted order
+        std::vector<std::vector<int>> key(R);
+        size_t direct = 0;
+        for (uint32_t j = 0; j < R; ++j)
+            for (int m : masks)
+                if ((int(j) & m) == m) { key[j].push_back(m); ++direct; }
+        std::map<std::vector<int>, std::string> node;
+        size_t trie = 0;
+        for (uint32_t j = 0; j < R; ++j) {
+            if (key[j].empty()) continue;
+            ++trie;
+            for (size_t len = 2; len <= key[j].size(); ++len)
+                if (node.emplace(std::vector<int>(key[j].begin(), key[j].begin() + len), std::string()).second) ++trie;
+        }
+        auto apply = [&](uint32_t j, const std::string& e) {
+            for (int s = 0; s < ns; ++s) {
+                const char* A = s ? "a1" : "a0";
+                o << "    " << A << "[" << j << "] = cmul(" << A << "[" << j << "], " << e << ");\n";
+            }
+        };
+        if (trie < direct) {
+            for (auto& kv : node) {   // map order: every prefix precedes its extensions
+                const std::vector<int>& k = kv.first;
+                const std::vector<int> parent(k.begin(), k.end() - 1);
+                const std::string pv = parent.size() == 1 ? val[parent[0]] : node[parent];
+                kv.second = "t" + std::to_string(nvar++);
+                o << "    const double2 " << kv.second << " = cmul(" << pv << ", " << val[k.back()] << ");\n";
+            }
+            for (uint32_t j = 0; j < R; ++j)
+                if (!key[j].empty()) apply(j, key[j].size() == 1 ? val[key[j][0]] : node[key[j]]);
+        } else {
+            for (int m : masks)
+                for (int s = 0; s < ns; ++s) {
+                    const char* A = s ? "a1" : "a0";
+                    if (m == 0) o << "    scaleAll(" << A << ", " << val[m] << ");\n";
+                    else o << "    phD<" << m << ">(" << A << ", " << val[m] << ");\n";
+                }
+        }
+        o << "  }\n";
+    }
+
     std::string run()
     {
         const uint32_t tsize = 1u << P.k;
         const uint32_t ng = uint32_t(P.groups.size());
         const uint32_t nslots = uint32_t(P.slot_src.size());
+
+        // the pass body first (it decides the lane tables the prologue builds)
+        set_layout(P.layouts[P.layout0]);
         std::ostringstream body;
         std::swap(o, body);
+        if (!P.acc_mul) emit_acc_decls();
+        for (const plan::KOp& op : P.ops) emit_op(op);
+        flush_run();
+        // store (final layout)
+        for (uint32_t j = 0; j < R; ++j) {
+            o << "  psi[gb + " << hex(reg_off(j)) << "] = a0[" << j << "];";
+            if (ns == 2) o << " lam[gb + " << hex(reg_off(j)) << "] = a1[" << j << "];";
+            o << "\n";
+        }
+        if (ns == 2 && nslots) {
+            o << "  __syncthreads();\n"
+              << "  for (u32 s = tid; s < " << nslots << "u; s += " << T << "u) { double v = 0.0;"
+              << " for (u32 w = 0; w < " << NW << "u; ++w) v += wp[s * " << NW << "u + w];"
+              << " slot_partial[(u64)s * gridDim.x + blockIdx.x] = v; }\n";
+        }
+        std::swap(o, body);
+        const std::string ops_txt = body.str();
+        set_layout(P.layouts[P.layout0]);
 
+        std::ostringstream head;
+        std::swap(o, head);
         o << "  const u32 tid = threadIdx.x;\n";
         o << "  extern __shared__ double2 sm[];\n";
         o << "  double2* xb = sm; (void)xb;\n";
         o << "  double2* gv = sm + " << tsize << "; (void)gv;\n";
-        if (ns == 2) o << "  double* wp = reinterpret_cast<double*>(gv + " << ng << ");\n";
+        o << "  double2* tb = gv + " << ng << "; (void)tb;\n";
+        if (ns == 2) o << "  double* wp = reinterpret_cast<double*>(tb + " << 32 * ntab << ");\n";
         // outer base
         o << "  u64 ob = 0;\n  { u64 c = blockIdx.x;";
         for (uint32_t q = 0; q < 64; ++q)
@@ -243,7 +434,19 @@ struct Gen {
             }
             o << "    return;\n  }\n";
         }
-        // prologue: per-CTA diagonal group values
+        // load first (gb holds only thread and outer bits, the offsets only
+        // register bits: gb + off == gb | off, and the constant folds into the
+        // address); the prologue below then runs while the loads are in flight
+        o << "  u64 gb = " << gbase_expr() << ";\n";
+        for (int s = 0; s < ns; ++s) o << "  double2 a" << s << "[" << R << "];\n";
+        if (!zero_in) {
+            for (uint32_t j = 0; j < R; ++j) {
+                o << "  a0[" << j << "] = psi[gb + " << hex(reg_off(j)) << "];";
+                if (ns == 2) o << " a1[" << j << "] = lam[gb + " << hex(reg_off(j)) << "];";
+                o << "\n";
+            }
+        }
+        // prologue: per-CTA diagonal group values, then the lane tables
         if (ng) {
             o << "  for (u32 g = tid; g < " << ng << "u; g += " << T << "u) {\n"
               << "    const GroupRec gr = groups[g]; double th = 0.0;\n"
@@ -251,39 +454,14 @@ struct Gen {
                  " if ((ob & t.ocond) == t.ocond) th += t.theta; }\n"
               << "    gv[g] = gr.direct ? expi(th) : make_double2(th, 0.0);\n  }\n";
         }
+        if (ntab) o << "  __syncthreads();\n" << tabs.str();
         if (ns == 2 && nslots) o << "  for (u32 i = tid; i < " << nslots * NW << "u; i += " << T << "u) wp[i] = 0.0;\n";
         o << "  __syncthreads();\n";
-        // load (gb holds only thread and outer bits, the offsets only register
-        // bits: gb + off == gb | off, and the constant folds into the address)
-        set_layout(P.layouts[P.layout0]);
-        o << "  u64 gb = " << gbase_expr() << ";\n";
-        for (int s = 0; s < ns; ++s) o << "  double2 a" << s << "[" << R << "];\n";
-        for (uint32_t j = 0; j < R; ++j) {
-            if (zero_in)
-                o << "  a0[" << j << "] = make_double2((gb | " << hex(reg_off(j)) << ") == 0ull ? 1.0 : 0.0, 0.0);";
-            else
-                o << "  a0[" << j << "] = psi[gb + " << hex(reg_off(j)) << "];";
-            if (ns == 2) o << " a1[" << j << "] = lam[gb + " << hex(reg_off(j)) << "];";
-            o << "\n";
-        }
-        emit_acc_decls();
+        if (zero_in)
+            for (uint32_t j = 0; j < R; ++j)
+                o << "  a0[" << j << "] = make_double2((gb | " << hex(reg_off(j)) << ") == 0ull ? 1.0 : 0.0, 0.0);\n";
+        std::swap(o, head);
 
-        for (const plan::KOp& op : P.ops) emit(op);
-
-        // store
-        for (uint32_t j = 0; j < R; ++j) {
-            o << "  psi[gb + " << hex(reg_off(j)) << "] = a0[" << j << "];";
-            if (ns == 2) o << " lam[gb + " << hex(reg_off(j)) << "] = a1[" << j << "];";
-            o << "\n";
-        }
-        if (ns == 2 && nslots) {
-            o << "  __syncthreads();\n"
-              << "  for (u32 s = tid; s < " << nslots << "u; s += " << T << "u) { double v = 0.0;"
-              << " for (u32 w = 0; w < " << NW << "u; ++w) v += wp[s * " << NW << "u + w];"
-              << " slot_partial[(u64)s * gridDim.x + blockIdx.x] = v; }\n";
-        }
-
-        std::swap(o, body);
         std::ostringstream src;
         src << kPrelude << "\n";
         src << "struct Prm { double v[" << std::max<size_t>(1, prm.size()) << "]; };\n";
@@ -293,7 +471,7 @@ struct Gen {
             << "double2* __restrict__ psi, double2* __restrict__ lam, const TermRec* __restrict__ terms, "
             << "const GroupRec* __restrict__ groups, double* __restrict__ slot_partial, const __grid_constant__ Prm P)\n{\n"
             << "  (void)lam; (void)terms; (void)groups; (void)slot_partial;\n"
-            << body.str() << "}\n";
+            << head.str() << ops_txt << "}\n";
         return src.str();
     }
 
@@ -470,7 +648,7 @@ Source generate(const plan::PassProgram& p, int nstates, bool zero_input)
     s.code = g.run();
     s.prm = std::move(g.prm);
     s.threads = g.T;
-    s.smem = (size_t(1) << p.k) * 16 + p.groups.size() * 16 +
+    s.smem = (size_t(1) << p.k) * 16 + p.groups.size() * 16 + size_t(g.ntab) * 32 * 16 +
              (nstates == 2 ? p.slot_src.size() * g.NW * 8 : 0);
     return s;
 }

@@ -114,7 +114,12 @@ public:
     // the current register bits; only when none is left does the pass change
     // register layout, to the bits with the most ready gates.  For the QFT
     // this halves the layouts of program order (one per block of register bits).
-    void run(const std::vector<Absorbed>& abs, double gphase)
+    // carry: constant factor deferred by the previous passes of the plan
+    // (the unscaled Hadamards' 1/sqrt2 and RZ's global phase); the pass
+    // applies carry times its own factor when it is the last pass (apply),
+    // else it applies nothing and returns the product for the next pass
+    std::pair<double, double> run(const std::vector<Absorbed>& abs, double gphase, std::pair<double, double> carry,
+                                  bool apply)
     {
         const int m = int(abs.size());
         std::vector<std::vector<int>> succ(m);
@@ -275,8 +280,15 @@ public:
             P.ops.push_back(op);
             P.n_nondiag++;
         }
-        if (opt_.keep_gphase) close_all(true, scale_ * std::cos(gphase_), scale_ * std::sin(gphase_));
-        else close_all(true, scale_, 0.0);
+        const double ga = opt_.keep_gphase ? scale_ * std::cos(gphase_) : scale_;
+        const double gb = opt_.keep_gphase ? scale_ * std::sin(gphase_) : 0.0;
+        const std::pair<double, double> c{carry.first * ga - carry.second * gb, carry.first * gb + carry.second * ga};
+        if (apply) {
+            close_all(true, c.first, c.second);
+            return {1.0, 0.0};
+        }
+        close_all(true, 1.0, 0.0);
+        return c;
     }
 
 private:
@@ -548,6 +560,10 @@ Plan build(const std::vector<Gate>& gates, uint32_t n, const uint32_t* perm_in, 
     plan.gates = gates.size();
     const uint32_t k = std::min<uint32_t>(opt.k, n);
     const uint32_t seed_bits = std::min<uint32_t>(3, k);
+    // forward plans defer every pass's constant factor to the last pass (no
+    // caller reads the state between the passes of one plan); gradient plans
+    // scale each pass, their K_GRAD_* weights assume it
+    std::pair<double, double> carry{1.0, 0.0};
 
     while (!remaining.empty()) {
         uint64_t T = 0;
@@ -609,7 +625,7 @@ Plan build(const std::vector<Gate>& gates, uint32_t n, const uint32_t* perm_in, 
         prog.outer_mask = all & ~T;
         prog.ngates = uint32_t(abs.size());
         Lowering low(prog, n, opt);
-        low.run(abs, gph);
+        carry = low.run(abs, gph, carry, opt.grads || deferred.empty());
         plan.passes.push_back(std::move(prog));
         remaining.swap(deferred);
     }
