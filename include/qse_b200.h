@@ -133,8 +133,9 @@ QSE_API const char* qse_version(void);
 QSE_API int qse_ctx_create(int device, qse_ctx** out);
 QSE_API int qse_ctx_destroy(qse_ctx* ctx);
 QSE_API int qse_ctx_synchronize(qse_ctx* ctx);
-/* fused-planner knobs: tile qubits (10..12), cap on gates per pass (0 = none),
- * fusion on/off (off = one kernel per gate, the plain method). */
+/* fused-planner knobs: tile qubits (10..12), cap on non-diagonal gates per pass
+ * (0 = none; with specialised pass kernels at most 256, which bounds their
+ * compile time), fusion on/off (off = one kernel per gate, the plain method). */
 QSE_API int qse_ctx_set_fusion(qse_ctx* ctx, int enabled, int tile_qubits, int max_gates_per_pass);
 /* 0 = sequential-rounding-exact CDF (default), 1 = plain parallel scan */
 QSE_API int qse_ctx_set_sample_mode(qse_ctx* ctx, int mode);
@@ -229,9 +230,9 @@ QSE_API int qse_plan_describe(uint32_t nqubits, const qse_op* ops, size_t nops, 
  * kernel and compiled for sm_100a at run time (cached by source); 0 = one
  * generic kernel interprets the pass program. */
 QSE_API int qse_ctx_set_jit(qse_ctx* ctx, int enabled);
-/* Generates and compiles (no GPU needed, nothing loaded) every pass kernel the
- * planner makes for ops: nstates 1 = forward passes, 2 = adjoint reverse
- * passes.  *source_bytes receives the total generated source size. */
+/* Generates and compiles (no GPU needed, nothing loaded) every distinct pass
+ * kernel the planner makes for ops: nstates 1 = forward passes, 2 = adjoint
+ * reverse passes.  *source_bytes receives the total generated source size. */
 QSE_API int qse_plan_compile(uint32_t nqubits, const qse_op* ops, size_t nops, const double* params,
                              size_t nparams, uint32_t tile_qubits, int nstates, size_t* source_bytes);
 

@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <set>
 #include <string>
 
 #include "jit.h"
@@ -594,16 +595,15 @@ int qse_plan_compile(uint32_t nqubits, const qse_op* ops, size_t nops, const dou
     opt.k = std::min<uint32_t>(tile_qubits ? tile_qubits : (nstates == 2 ? 11 : 12), nqubits);
     opt.grads = nstates == 2;
     opt.acc_mul = true;
-    if (nstates == 2) {
-        opt.max_terms = 512;
-        opt.max_gates = 256;
-    }
+    opt.max_gates = qse::plan::kJitMaxGates;
+    if (nstates == 2) opt.max_terms = 512;
     qse::plan::Plan pl = qse::plan::build(gates, nqubits, perm, opt);
     size_t total = 0;
+    std::set<std::string> done;   // identical passes share one kernel, as in execution
     for (const auto& p : pl.passes) {
         qse::jit::Source s = qse::jit::generate(p, nstates);
         total += s.code.size();
-        qse::jit::compile_only(s);
+        if (done.insert(s.code).second) qse::jit::compile_only(s);
     }
     if (source_bytes) *source_bytes = total;
     QSE_GUARD_END

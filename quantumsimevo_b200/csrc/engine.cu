@@ -162,26 +162,53 @@ Uploaded upload_plan(qse_ctx* ctx, const plan::Plan& pl)
     return up;
 }
 
-// Runs the passes of a plan: specialised NVRTC kernels (jit.cpp) when the
-// context allows it, else the generic tile-program interpreter (tile.cu).
+// Specialised pass kernels repay their compile time (NVRTC: about a second or
+// more per distinct kernel) when a pass is expensive, i.e. on large states, or
+// when few of a plan's kernels are new.  A deep circuit on a small state can
+// need hundreds of distinct kernels; its plan runs on the interpreter instead.
+constexpr uint32_t kJitAlwaysQubits = 22;
+constexpr size_t kJitMaxNewKernels = 32;
+
+// Plans gates for the specialised kernels (their sources generated into srcs,
+// use_jit = true) or, when the context disables them or they are not worth
+// compiling, for the interpreter (angle accumulators, use_jit = false).
+plan::Plan plan_for(qse_state* st, const std::vector<plan::Gate>& gates, plan::Options opt, int ns, bool& use_jit,
+                    std::vector<jit::Source>& srcs)
+{
+    use_jit = st->ctx->jit != 0;
+    opt.acc_mul = use_jit;
+    plan::Plan pl = plan::build(gates, st->n, st->perm, opt);
+    srcs.clear();
+    if (!use_jit) return pl;
+    srcs.reserve(pl.passes.size());
+    for (size_t i = 0; i < pl.passes.size(); ++i)
+        srcs.push_back(jit::generate(pl.passes[i], ns, i == 0 && ns == 1 && st->lazy_zero));
+    if (st->n >= kJitAlwaysQubits || jit::count_uncached(srcs) <= kJitMaxNewKernels) return pl;
+    use_jit = false;
+    srcs.clear();
+    opt.acc_mul = false;
+    return plan::build(gates, st->n, st->perm, opt);
+}
+
+// Runs the passes of a plan: specialised NVRTC kernels (jit.cpp, sources from
+// plan_for) or the generic tile-program interpreter (tile.cu).
 struct PassRunner {
     qse_ctx* ctx;
     qse_state* st;
     Uploaded& up;
     int ns;
     uint32_t rb;
+    bool jit;
     std::vector<jit::Source> srcs;
     std::vector<std::shared_ptr<jit::Kernel>> ks;
     std::vector<uint32_t> kq;
 
-    PassRunner(qse_state* s, const plan::Plan& pl, Uploaded& u, int nstates, uint32_t regbits)
-        : ctx(s->ctx), st(s), up(u), ns(nstates), rb(regbits)
+    PassRunner(qse_state* s, const plan::Plan& pl, Uploaded& u, int nstates, uint32_t regbits, bool use_jit,
+               std::vector<jit::Source>&& sources)
+        : ctx(s->ctx), st(s), up(u), ns(nstates), rb(regbits), jit(use_jit), srcs(std::move(sources))
     {
         for (const auto& p : pl.passes) kq.push_back(p.k);
-        if (!ctx->jit) return;
-        srcs.reserve(pl.passes.size());
-        for (size_t i = 0; i < pl.passes.size(); ++i)
-            srcs.push_back(jit::generate(pl.passes[i], ns, i == 0 && ns == 1 && s->lazy_zero));
+        if (!jit) return;
         std::vector<const jit::Source*> ptrs;
         for (const auto& s2 : srcs) ptrs.push_back(&s2);
         ks = jit::get_kernels(ptrs);
@@ -193,7 +220,7 @@ struct PassRunner {
         a.psi = reinterpret_cast<double2*>(st->amp);
         a.lam = lam;
         a.slot_partial = part;
-        if (!ctx->jit) {
+        if (!jit) {
             tile::launch_pass(ctx, a, st->n, rb, ns);
             return;
         }
@@ -279,10 +306,13 @@ void execute_program(qse_state* st, const qse_op* ops, size_t nops, const double
         opt.rb = 4;
         opt.k = tile_qubits_for(ctx, st->n, 4, 12);
         opt.max_gates = uint32_t(std::max(0, ctx->max_gates_per_pass));
-        opt.acc_mul = ctx->jit != 0;
-        plan::Plan pl = plan::build(gates, st->n, st->perm, opt);
+        if (ctx->jit && (opt.max_gates == 0 || opt.max_gates > plan::kJitMaxGates)) opt.max_gates = plan::kJitMaxGates;
+        bool use_jit = false;
+        std::vector<jit::Source> srcs;
+        plan::Plan pl = plan_for(st, gates, opt, 1, use_jit, srcs);
+        if (!use_jit) materialize(st);  // interpreter passes read the state
         Uploaded up = upload_plan(ctx, pl);
-        PassRunner runner(st, pl, up, 1, 4);
+        PassRunner runner(st, pl, up, 1, 4, use_jit, std::move(srcs));
         for (size_t i = 0; i < up.args.size(); ++i) runner.run(i, nullptr, nullptr);
         if (!up.args.empty()) st->lazy_zero = false;  // the first pass wrote every amplitude
         for (uint32_t q = 0; q < st->n; ++q) st->perm[q] = pl.perm_final[q];
@@ -489,10 +519,11 @@ double adjoint(qse_state* st, const qse_op* ops, size_t nops, const double* para
     opt.rb = 3;
     opt.k = tile_qubits_for(ctx, st->n, 3, 11);
     opt.grads = true;
-    opt.acc_mul = ctx->jit != 0;
     opt.max_terms = 512;
-    opt.max_gates = 256;
-    plan::Plan pl = plan::build(rev, st->n, st->perm, opt);
+    opt.max_gates = plan::kJitMaxGates;
+    bool use_jit = false;
+    std::vector<jit::Source> srcs;
+    plan::Plan pl = plan_for(st, rev, opt, 2, use_jit, srcs);
     Uploaded up = upload_plan(ctx, pl);
 
     // occurrence gradients accumulate in scratch2: [nops] | slot partials
@@ -517,7 +548,7 @@ double adjoint(qse_state* st, const qse_op* ops, size_t nops, const double* para
             std::memcpy(h + i * b_src, pl.passes[i].slot_src.data(), pl.passes[i].slot_src.size() * 4);
         QSE_CUDA(cudaMemcpyAsync(srcbase, h, b_src * pl.passes.size(), cudaMemcpyHostToDevice, ctx->stream));
     }
-    PassRunner runner(st, pl, up, 2, 3);
+    PassRunner runner(st, pl, up, 2, 3, use_jit, std::move(srcs));
     for (size_t i = 0; i < up.args.size(); ++i) {
         const tile::PassArgs& a = up.args[i];
         runner.run(i, reinterpret_cast<double2*>(st->aux), part);

@@ -23,7 +23,9 @@
 #include <memory>
 #include <mutex>
 #include <sstream>
+#include <string_view>
 #include <thread>
+#include <unordered_set>
 
 namespace qse {
 namespace jit {
@@ -651,6 +653,16 @@ Source generate(const plan::PassProgram& p, int nstates, bool zero_input)
     s.smem = (size_t(1) << p.k) * 16 + p.groups.size() * 16 + size_t(g.ntab) * 32 * 16 +
              (nstates == 2 ? p.slot_src.size() * g.NW * 8 : 0);
     return s;
+}
+
+size_t count_uncached(const std::vector<Source>& srcs)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    std::unordered_set<std::string_view> seen;
+    size_t n = 0;
+    for (const Source& s : srcs)
+        if (g_cache.find(s.code) == g_cache.end() && seen.insert(s.code).second) ++n;
+    return n;
 }
 
 std::vector<std::shared_ptr<Kernel>> get_kernels(const std::vector<const Source*>& srcs)

@@ -34,6 +34,8 @@ size_t compile_only(const Source& s);
 // zero_input: the state is |0..0> (not in memory); the pass generates its
 // input amplitudes instead of loading them (forward passes only)
 Source generate(const plan::PassProgram& p, int nstates, bool zero_input = false);
+// distinct sources among srcs that are not compiled yet
+size_t count_uncached(const std::vector<Source>& srcs);
 // compiled kernels for every source (cached by source text; missing ones are compiled in parallel)
 std::vector<std::shared_ptr<Kernel>> get_kernels(const std::vector<const Source*>& srcs);
 void launch(qse_ctx* ctx, Kernel& k, const Source& s, uint32_t n, uint32_t kq, void* psi, void* lam,

@@ -22,6 +22,10 @@ namespace plan {
 namespace {
 
 constexpr double kInvSqrt2 = 0.7071067811865475244;  // CircuitUnitaryOperation.cpp:87
+// smallest pending scale (unscaled Hadamards, deferred pass constants) before it
+// is applied: stored values stay below 2^200 times the state's own, and a pass
+// adds at most another 2^200, far from the 2^1024 overflow
+constexpr double kFlushScale = 0x1p-200;
 
 enum Cls { C_DROP, C_N1, C_CX, C_DIAG, C_SWAP };
 
@@ -279,11 +283,19 @@ public:
             }
             P.ops.push_back(op);
             P.n_nondiag++;
+            // each unscaled Hadamard grows the stored values by sqrt2: apply the
+            // pending 1/sqrt2 factors before they fall below kFlushScale
+            if (scale_ < kFlushScale) {
+                close_all(true, scale_, 0.0);
+                scale_ = 1.0;
+            }
         }
         const double ga = opt_.keep_gphase ? scale_ * std::cos(gphase_) : scale_;
         const double gb = opt_.keep_gphase ? scale_ * std::sin(gphase_) : 0.0;
         const std::pair<double, double> c{carry.first * ga - carry.second * gb, carry.first * gb + carry.second * ga};
-        if (apply) {
+        // the deferred constant stays above kFlushScale in magnitude, so the
+        // stored amplitudes stay below 1 / kFlushScale times their true size
+        if (apply || std::hypot(c.first, c.second) < kFlushScale) {
             close_all(true, c.first, c.second);
             return {1.0, 0.0};
         }

@@ -120,6 +120,12 @@ struct Gate {
     int32_t grad = -1;     // gradient occurrence id (adjoint reverse sweep), -1 = none
 };
 
+// Non-diagonal gates per pass when the passes are compiled into specialised
+// kernels: NVRTC's compile time grows faster than linearly with the length of
+// the straight-line kernel (a 12-qubit pass of 2400 gates takes over a minute),
+// while an extra pass costs one sweep of the state.
+constexpr uint32_t kJitMaxGates = 256;
+
 struct Options {
     uint32_t k = 12;             // tile qubits (clamped to n)
     uint32_t rb = 4;             // register bits per thread
