@@ -176,6 +176,35 @@ __device__ uint64_t block_scan_add(uint64_t v, uint64_t& excl, uint64_t* sh)
     return total;
 }
 
+// block_scan_add on integer-valued doubles; exact while the sums stay below 2^53
+__device__ double block_scan_addd(double v, double& excl, double* sh)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nw = blockDim.x >> 5;
+    double inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += u;
+    }
+    if (lane == 31) sh[warp] = inc;
+    __syncthreads();
+    if (tid == 0) {
+        double run = 0.0;
+        for (int w = 0; w < nw; ++w) {
+            const double t = sh[w];
+            sh[32 + w] = run;
+            run += t;
+        }
+        sh[64] = run;
+    }
+    __syncthreads();
+    excl = sh[32 + warp] + (inc - v);
+    const double total = sh[64];
+    __syncthreads();
+    return total;
+}
+
 __device__ __forceinline__ void compose(uint64_t a0, uint64_t a1, uint64_t b0, uint64_t b1, uint64_t& r0, uint64_t& r1)
 {
     // first a, then b
@@ -228,17 +257,73 @@ __device__ void block_scan_maps(uint64_t t0, uint64_t t1, uint64_t& ex0, uint64_
 }
 
 // Exact sequential cumulative sums of one block of `cnt` (<= kBS) values held
-// as p[0..kEPT) per thread (element index = tid*kEPT + j), starting from the
-// exact running sum c_in.  Writes the values to out (if non-null) and returns
-// the block's final sum.  Must be called by all threads of the block.
-__device__ __forceinline__ double block_exact(const double (&p)[kEPT], uint32_t cnt, double c_in, double* out, uint64_t* sh,
-                              double* stage)
+// in stage (element i at stage_slot(i), so thread tid's elements tid*kEPT + j
+// sit in row tid), starting from the exact running sum c_in.  The values go
+// to out (if non-null), staged in the same buffer.  Returns the block's final
+// sum.  Must be called by all threads of the block.
+__device__ __forceinline__ double block_exact(uint32_t cnt, double c_in, double* out, uint64_t* sh, double* stage)
 {
     __shared__ double s_c;
     __shared__ int s_t;
     const uint32_t tid = threadIdx.x;
     uint32_t pos = 0;
     double c = c_in;
+    // Fast path (nearly every block): a full block on a fast grid with no tie
+    // and a running sum that stays below 2^53 grid units.  The grid integers
+    // and all their partial sums are then exact in FP64, so the scan runs on
+    // doubles with no integer conversion; otherwise fall through.
+    if (cnt == uint32_t(kBS) && c > 0.0) {
+        const int e = epoch_of(c);
+        const Grid g = grid_of(e);
+        if (g.fast) {
+            double q[kEPT];
+            double tsum = 0.0;
+            bool ok = true;
+#pragma unroll
+            for (int j = 0; j < kEPT; ++j) {
+                const double pj = stage[tid * kPad + j];
+                const double x = pj * g.scale;
+                const double r = rint(x);
+                const double df = x - r;
+                ok = ok && pj < g.limit && df != 0.5 && df != -0.5;
+                q[j] = r;
+                tsum += r;
+            }
+            if (__syncthreads_and(ok)) {
+                double ex;
+                block_scan_addd(tsum, ex, reinterpret_cast<double*>(sh));
+                double run = c * g.scale + ex;
+#pragma unroll
+                for (int j = 0; j < kEPT; ++j) {
+                    run += q[j];
+                    q[j] = run;
+                }
+                if (!__syncthreads_or(run >= 0x1p53)) {   // sums only grow: the last is the largest
+                    const double G = ldexp(1.0, e - 52);
+                    if (out) {
+#pragma unroll
+                        for (int j = 0; j < kEPT; ++j) stage[tid * kPad + j] = q[j] * G;
+                    }
+                    if (tid == blockDim.x - 1) s_c = run * G;
+                    __syncthreads();
+                    if (out) {
+#pragma unroll
+                        for (int j = 0; j < kEPT; ++j) {
+                            const uint32_t i = j * kBT + tid;
+                            out[i] = stage[stage_slot(i)];
+                        }
+                    }
+                    const double cf = s_c;
+                    __syncthreads();
+                    return cf;
+                }
+            }
+        }
+    }
+    // general path (the fast path writes stage only when it returns)
+    double p[kEPT];
+#pragma unroll
+    for (int j = 0; j < kEPT; ++j) p[j] = stage[tid * kPad + j];
     while (pos < cnt) {
         const int e = epoch_of(c);
         const double G = ldexp(1.0, e - 52);
@@ -322,10 +407,9 @@ __device__ __forceinline__ double block_exact(const double (&p)[kEPT], uint32_t 
         // step t with a real FP64 addition (the reference's own rounding)
         if (tid == t / kEPT) {
             double prev = s_c;
-            double pt = 0.0;
-#pragma unroll
-            for (int j = 0; j < kEPT; ++j)
-                if (j == int(t % kEPT)) pt = p[j];
+            // element t from the staging buffer: slots >= t are still the
+            // probabilities (indexing p[] here would put it in local memory)
+            const double pt = stage[stage_slot(t)];
             double ct = __dadd_rn(prev, pt);
             if (out) stage[stage_slot(t)] = ct;
             s_c = ct;
@@ -474,71 +558,132 @@ __global__ void __launch_bounds__(kBT) k_prob_gather(const double2* __restrict__
     }
 }
 
-// single CTA: approximate exclusive prefix -> grid guess per block
-__global__ void __launch_bounds__(1024) k_cdf_guess(const double* __restrict__ bsum, uint32_t nb, int32_t* guess)
+// Grid guess per block from approximate prefix sums of the block sums, in
+// groups of kGT blocks: k_guess_part sums each group, k_guess_fin adds the
+// groups before its own and scans its group.  The guess only selects the
+// binades k_cdf_summ folds on; a block whose exact running sum turns out to
+// lie elsewhere is folded exactly by the chain, so the summation order here
+// affects speed, never results.
+constexpr int kGT = 1024;
+
+__device__ __forceinline__ double block_sum_all(double v, double* sh)
 {
-    __shared__ double part[1024];
-    const uint32_t per = (nb + blockDim.x - 1) / blockDim.x;
-    const uint32_t lo = threadIdx.x * per, hi = min(nb, lo + per);
-    double s = 0.0;
-    for (uint32_t b = lo; b < hi; ++b) s += bsum[b];
-    part[threadIdx.x] = s;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     __syncthreads();
-    if (threadIdx.x == 0) {
-        double run = 0.0;
-        for (uint32_t t = 0; t < blockDim.x; ++t) {
-            double v = part[t];
-            part[t] = run;
-            run += v;
-        }
-    }
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
     __syncthreads();
-    double run = part[threadIdx.x];
-    for (uint32_t b = lo; b < hi; ++b) {
-        double lo_c = run, hi_c = run + bsum[b];
-        // conservative slack for the difference between this sum and the sequential one
-        double slack = hi_c * 0x1.0p-20 + 1e-300;
-        int e1 = lo_c - slack > 2.2250738585072014e-308 ? ilogb(lo_c - slack) : -1022;
-        int e2 = hi_c + slack > 2.2250738585072014e-308 ? ilogb(hi_c + slack) : -1022;
-        // 2 e1 + 1 when the block may reach binade e1 + 1, 2 e1 when it stays in e1
-        guess[b] = (e2 - e1 <= 1) ? 2 * e1 + (e2 - e1) : INT32_MIN;
-        run = hi_c;
-    }
+    double t = 0.0;
+    for (uint32_t w = 0; w < (blockDim.x >> 5); ++w) t += sh[w];
+    return t;
 }
 
-__global__ void __launch_bounds__(kBT) k_cdf_summ(const double* __restrict__ prob,
-                                                  const int32_t* __restrict__ guess, Summ* __restrict__ summ)
+__global__ void __launch_bounds__(kGT) k_guess_part(const double* __restrict__ bsum, uint32_t nb,
+                                                    double* __restrict__ gtot)
 {
-    __shared__ uint64_t sh[160];
-    const int32_t gs = guess[blockIdx.x];
-    if (gs == INT32_MIN) {
-        if (threadIdx.x == 0) summ[blockIdx.x] = Summ{{{0, 0}, {0, 0}}, gs, 0};
-        return;
+    __shared__ double sh[32];
+    const uint32_t b = blockIdx.x * kGT + threadIdx.x;
+    const double t = block_sum_all(b < nb ? bsum[b] : 0.0, sh);
+    if (threadIdx.x == 0) gtot[blockIdx.x] = t;
+}
+
+__global__ void __launch_bounds__(kGT) k_guess_fin(const double* __restrict__ bsum, uint32_t nb,
+                                                   const double* __restrict__ gtot, int32_t* __restrict__ guess)
+{
+    __shared__ double sh[32];
+    __shared__ double wsc[32];
+    double o = 0.0;
+    for (uint32_t g = threadIdx.x; g < blockIdx.x; g += kGT) o += gtot[g];
+    o = block_sum_all(o, sh);
+    const uint32_t b = blockIdx.x * kGT + threadIdx.x;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const double v = b < nb ? bsum[b] : 0.0;
+    double inc = v;
+    for (int d = 1; d < 32; d <<= 1) {
+        const double u = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= uint32_t(d)) inc += u;
     }
+    if (lane == 31) wsc[warp] = inc;
+    __syncthreads();
+    double wo = 0.0;
+    for (uint32_t w = 0; w < warp; ++w) wo += wsc[w];
+    if (b >= nb) return;
+    const double lo_c = o + wo + (inc - v), hi_c = o + wo + inc;
+    // conservative slack for the difference between this sum and the sequential one
+    const double slack = hi_c * 0x1.0p-20 + 1e-300;
+    const int e1 = lo_c - slack > 2.2250738585072014e-308 ? ilogb(lo_c - slack) : -1022;
+    const int e2 = hi_c + slack > 2.2250738585072014e-308 ? ilogb(hi_c + slack) : -1022;
+    // 2 e1 + 1 when the block may reach binade e1 + 1, 2 e1 when it stays in e1
+    guess[b] = (e2 - e1 <= 1) ? 2 * e1 + (e2 - e1) : INT32_MIN;
+}
+
+// Block b's probabilities into the padded staging buffer with asynchronous
+// 8-byte copies (same slots as load_block_prob), committed as one group; the
+// persistent k_cdf_write fetches the next block while it works on this one.
+__device__ __forceinline__ void stage_async(double* stage, const double* prob, uint64_t base)
+{
+#pragma unroll
+    for (int j = 0; j < kEPT; ++j) {
+        const uint32_t i = j * kBT + threadIdx.x;
+        const uint32_t sa = uint32_t(__cvta_generic_to_shared(stage + stage_slot(i)));
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(prob + base + i) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void stage_wait()
+{
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+// shared memory of k_cdf_write: two staging buffers
+constexpr size_t kStage2 = size_t(2) * kBT * kPad * sizeof(double);
+// resident CTAs per SM of k_cdf_write (its register budget: 128 per thread);
+// the persistent grid is exactly that many per SM
+constexpr int kWriteCTAs = 2;
+
+// fold of one block on the one or two binades its guess allows
+__device__ __forceinline__ Summ block_summ(const double (&p)[kEPT], int32_t gs, uint64_t* sh)
+{
     const int32_t e = gs >> 1;          // arithmetic shift: floor(gs / 2)
     const int nbin = 1 + (gs & 1);      // binades the block may run in
-    __shared__ double stage[kBT * kPad];
-    double p[kEPT];
-    load_block_prob(prob, uint64_t(blockIdx.x) * kBS, p, stage);
     Summ out{{{0, 0}, {0, 0}}, e, 0};
     for (int k = 0; k < nbin; ++k) {
         const Grid g = grid_of(e + k);
         int ok = 1;
         bool pure = true;
-        uint64_t tsum = 0;
+        double tsum = 0.0;
+        if (g.fast) {
+            // grid integers as doubles (exact below 2^53; a larger total
+            // means the block leaves the binade, whatever its exact value)
 #pragma unroll
-        for (int j = 0; j < kEPT; ++j) {
-            uint64_t a0, a1;
-            if (!elem_map_g(p[j], g, a0, a1)) ok = 0;
-            pure = pure && a0 == a1;
-            tsum += a0;
+            for (int j = 0; j < kEPT; ++j) {
+                const double x = p[j] * g.scale;
+                const double r = rint(x);
+                const double df = x - r;
+                if (!(p[j] < g.limit)) ok = 0;
+                pure = pure && df != 0.5 && df != -0.5;
+                tsum += r;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < kEPT; ++j) {
+                uint64_t a0, a1;
+                if (!elem_map_g(p[j], g, a0, a1)) ok = 0;
+                pure = pure && a0 == a1;
+                tsum += double(a0);
+            }
         }
         const int both = __syncthreads_and(ok) | (__syncthreads_and(pure) << 1);
         if (!(both & 1)) continue;  // an element leaves binade e+k by itself: no fold there
         if (both & 2) {
-            uint64_t ex;
-            const uint64_t total = block_scan_add(tsum, ex, sh);
-            out.d[k][0] = out.d[k][1] = total;
+            double* shd = reinterpret_cast<double*>(sh);
+            for (int o = 16; o > 0; o >>= 1) tsum += __shfl_xor_sync(0xffffffffu, tsum, o);
+            if ((threadIdx.x & 31) == 0) shd[threadIdx.x >> 5] = tsum;
+            __syncthreads();
+            double total = 0.0;
+            for (int w = 0; w < kBT / 32; ++w) total += shd[w];
+            __syncthreads();
+            const uint64_t d = total >= 0x1p53 ? kTwo53 : uint64_t(total);
+            out.d[k][0] = out.d[k][1] = d;
         } else {
             uint64_t t0 = 0, t1 = 0;
 #pragma unroll
@@ -558,6 +703,22 @@ __global__ void __launch_bounds__(kBT) k_cdf_summ(const double* __restrict__ pro
         }
         out.ok |= 1 << k;
     }
+    return out;
+}
+
+__global__ void __launch_bounds__(kBT) k_cdf_summ(const double* __restrict__ prob,
+                                                  const int32_t* __restrict__ guess, Summ* __restrict__ summ)
+{
+    __shared__ uint64_t sh[160];
+    const int32_t gs = guess[blockIdx.x];
+    if (gs == INT32_MIN) {
+        if (threadIdx.x == 0) summ[blockIdx.x] = Summ{{{0, 0}, {0, 0}}, gs, 0};
+        return;
+    }
+    __shared__ double stage[kBT * kPad];
+    double p[kEPT];
+    load_block_prob(prob, uint64_t(blockIdx.x) * kBS, p, stage);
+    const Summ out = block_summ(p, gs, sh);
     if (threadIdx.x == blockDim.x - 1) summ[blockIdx.x] = out;
 }
 
@@ -582,7 +743,56 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double* __restrict__ pr
     // the binade it actually starts in, else an exact element-by-element
     // fold) and the scan restarts after it.
     __shared__ int s_end;
-    for (uint32_t base = 0; base < nb; base += kBT) {
+    uint32_t base = 0;
+    while (base < nb) {
+        // Super-chunk of 4 kBT blocks, 4 consecutive per thread, taken whole
+        // when every block has a fold on the running sum's binade and the sum
+        // stays in it (nearly always); else the chunks below redo it.
+        if (base + 4 * kBT <= nb) {
+            const double c = s_c;
+            const int e0 = epoch_of(c);
+            uint64_t d0[4], d1[4];
+            bool good = c > 0.0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                d0[k] = d1[k] = 0;
+                good = summ_pick(summ[base + 4 * t + k], e0, d0[k], d1[k]) && good;
+            }
+            if (__syncthreads_and(good)) {
+                uint64_t m0 = 0, m1 = 0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    uint64_t r0, r1;
+                    compose(m0, m1, d0[k], d1[k], r0, r1);
+                    m0 = r0;
+                    m1 = r1;
+                }
+                uint64_t ex0, ex1;
+                if (__syncthreads_and(m0 == m1)) {
+                    block_scan_add(m0, ex0, sh);
+                    ex1 = ex0;
+                } else {
+                    block_scan_maps(m0, m1, ex0, ex1, sh);
+                }
+                const uint64_t C = uint64_t(ldexp(c, 52 - e0));
+                uint64_t x = C + ((C & 1) ? ex1 : ex0);
+                uint64_t xin[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    xin[k] = x;
+                    x += (x & 1) ? d1[k] : d0[k];
+                }
+                if (!__syncthreads_or(x >= kTwo53)) {   // sums only grow: the last is the largest
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) cin[base + 4 * t + k] = ldexp(double(xin[k]), e0 - 52);
+                    if (t == kBT - 1) s_c = ldexp(double(x), e0 - 52);
+                    ++n_fast;
+                    __syncthreads();
+                    base += 4 * kBT;
+                    continue;
+                }
+            }
+        }
         const uint32_t cnt = min(uint32_t(kBT), nb - base);
         uint32_t pos = 0;
         while (pos < cnt) {
@@ -641,11 +851,12 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double* __restrict__ pr
                 ++n_exact;
                 double p[kEPT];
                 load_block_prob(prob, uint64_t(b) * kBS, p, stage);
-                double cc = block_exact(p, kBS, s_c, nullptr, sh, stage);
+                double cc = block_exact(kBS, s_c, nullptr, sh, stage);
                 if (t == 0) s_c = cc;
             }
             __syncthreads();
         }
+        base += kBT;
     }
     if (t == 0) {
         cin[nb] = s_c;
@@ -658,14 +869,31 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double* __restrict__ pr
     }
 }
 
-// in place: the probabilities of each block are replaced by their exact cumulative sums
-__global__ void __launch_bounds__(kBT) k_cdf_write(const double* __restrict__ cin, double* __restrict__ cdf)
+// in place: the probabilities of each block are replaced by their exact
+// cumulative sums.  Persistent: blocks blockIdx.x, +gridDim.x, ...; the next
+// block's probabilities stream into the other staging buffer meanwhile, and a
+// block's own buffer then stages its output for the coalesced copy.
+__global__ void __launch_bounds__(kBT, kWriteCTAs) k_cdf_write(const double* __restrict__ cin,
+                                                               double* __restrict__ cdf, uint32_t nb)
 {
     __shared__ uint64_t sh[160];
-    __shared__ double stage[kBT * kPad];
-    double p[kEPT];
-    load_block_prob(cdf, uint64_t(blockIdx.x) * kBS, p, stage);
-    block_exact(p, kBS, cin[blockIdx.x], cdf + uint64_t(blockIdx.x) * kBS, sh, stage);
+    extern __shared__ double stg[];
+    uint32_t b = blockIdx.x;
+    if (b >= nb) return;
+    stage_async(stg, cdf, uint64_t(b) * kBS);
+    for (uint32_t it = 0; b < nb; b += gridDim.x, ++it) {
+        double* cur = stg + (it & 1) * (kBT * kPad);
+        const uint32_t bn = b + gridDim.x;
+        if (bn < nb) {
+            stage_async(stg + ((it + 1) & 1) * (kBT * kPad), cdf, uint64_t(bn) * kBS);
+            stage_wait<1>();
+        } else {
+            stage_wait<0>();
+        }
+        __syncthreads();
+        block_exact(kBS, cin[b], cdf + uint64_t(b) * kBS, sh, cur);
+        __syncthreads();  // cur is refilled by the next iteration's prefetch
+    }
 }
 
 // small states (< one block): the sequential chain itself
@@ -823,17 +1051,19 @@ CdfView build_cdf(qse_state* st)
         count_launch(ctx);
     } else {
         const uint32_t nb = uint32_t(size / kBS);
-        // state-owned: cdf [size] | cin [nb+1];  context scratch: bsum [nb] | guess [nb] | summ [nb]
+        // state-owned: cdf [size] | cin [nb+1];  context scratch: bsum [nb] | guess [nb] | summ [nb] | group sums
         st->cdf.reserve(size * 8 + (size_t(nb) + 1) * 8 + 16);
         v.cdf = static_cast<double*>(st->cdf.ptr);
         v.cin = v.cdf + size;
         size_t off_guess = size_t(nb) * 8;
         size_t off_summ = (off_guess + size_t(nb) * 4 + 15) & ~size_t(15);
-        ctx->scratch2.reserve(off_summ + size_t(nb) * sizeof(Summ));
+        size_t off_gtot = off_summ + size_t(nb) * sizeof(Summ);
+        ctx->scratch2.reserve(off_gtot + (size_t(nb) / kGT + 1) * 8);
         char* base = static_cast<char*>(ctx->scratch2.ptr);
         double* bsum = reinterpret_cast<double*>(base);
         int32_t* guess = reinterpret_cast<int32_t*>(base + off_guess);
         Summ* summ = reinterpret_cast<Summ*>(base + off_summ);
+        double* gtot = reinterpret_cast<double*>(base + off_gtot);
         v.nb = nb;
         v.bs = kBS;
         // probabilities in logical order into the cumulative array (transformed in place below)
@@ -846,12 +1076,17 @@ CdfView build_cdf(qse_state* st)
             k_prob_gather<<<unsigned(size / kBS), kBT, 0, ctx->stream>>>(amp, v.cdf, bsum, g);
             count_launch(ctx);
         }
-        k_cdf_guess<<<1, 1024, 0, ctx->stream>>>(bsum, nb, guess);
+        const uint32_t ng = (nb + kGT - 1) / kGT;
+        k_guess_part<<<ng, kGT, 0, ctx->stream>>>(bsum, nb, gtot);
+        k_guess_fin<<<ng, kGT, 0, ctx->stream>>>(bsum, nb, gtot, guess);
         k_cdf_summ<<<nb, kBT, 0, ctx->stream>>>(v.cdf, guess, summ);
         k_cdf_chain<<<1, kBT, 0, ctx->stream>>>(v.cdf, summ, nb, v.cin, reinterpret_cast<uint32_t*>(v.cin + nb + 1));
-        k_cdf_write<<<nb, kBT, 0, ctx->stream>>>(v.cin, v.cdf);
+        // the attribute belongs to the current device: set on every build
+        QSE_CUDA(cudaFuncSetAttribute(k_cdf_write, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kStage2)));
+        const unsigned pgrid = unsigned(std::min<uint64_t>(nb, uint64_t(ctx->num_sms) * kWriteCTAs));
+        k_cdf_write<<<pgrid, kBT, kStage2, ctx->stream>>>(v.cin, v.cdf, nb);
         QSE_CUDA(cudaGetLastError());
-        count_launch(ctx, 4);
+        count_launch(ctx, 5);
     }
     st->cdf_values = v.cdf;
     st->cdf_block_start = v.cin;

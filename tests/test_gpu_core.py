@@ -213,6 +213,19 @@ def test_sample_bit_exact(dev, n):
     assert np.array_equal(_sample_on(dev, n, st, u), O.sample(st, n, u))
 
 
+@pytest.mark.parametrize("spread", [0.0, 40.0])
+def test_sample_bit_exact_many_blocks(dev, spread):
+    # 2048 blocks of 4096: every persistent CTA of the CDF write takes several
+    # blocks and the chain several 1024-block chunks; spread > 0 puts the
+    # magnitudes over many binades so the slow paths run inside those loops
+    n = 23
+    rng = np.random.default_rng(23 + int(spread))
+    amp = (rng.standard_normal(1 << n) + 1j * rng.standard_normal(1 << n)) * np.exp(-rng.uniform(0, spread, 1 << n))
+    amp /= np.linalg.norm(amp)
+    u = boundary_uniforms(amp, n, 400, 4)
+    assert np.array_equal(_sample_on(dev, n, amp, u), O.sample(amp, n, u))
+
+
 @pytest.mark.parametrize("n", [5, 14, 18])
 def test_sample_after_execute(dev, n):
     # end to end: outcomes equal the oracle's sampler on the device state; against the
