@@ -33,6 +33,15 @@
 #include "CircuitUnitaryOperationB200.h"
 #endif
 
+#ifdef QSE_REF_WITH_PLAYGROUND
+#include "QFT.h"
+// Grover::createGroverCircuit is a private static member; the test shim
+// calls it directly (it builds the circuit without running or printing)
+#define private public
+#include "Grover.h"
+#undef private
+#endif
+
 static int g_backend = 0;
 
 std::unique_ptr<ICircuitUnitaryOperation> CircuitUnitaryOperationFactory::create(size_t numQubits)
@@ -155,6 +164,31 @@ void ref_circuit_state(void* h, double* out)
     }
     auto& v = rc->c->getStateVector().data();
     std::memcpy(out, v.data(), v.size() * sizeof(std::complex<double>));
+}
+
+// The reference playground's circuit builders queueing onto a reference
+// Circuit, with the preamble of the run* function that calls them:
+// which 0 = QFT::runQFT (QFT.cpp:39-71: X(0), createQFT over 0..n-1),
+// 1 = QFT::runIQFT (QFT.cpp:73-105: X(0), createIQFT), 2 =
+// Grover::createGroverCircuit(n, target, iterations) (Grover.cpp:65-75).
+// Returns -1 when built without the playground sources or for an unknown which.
+int ref_playground_build(void* h, int which, int target, int iterations)
+{
+#ifdef QSE_REF_WITH_PLAYGROUND
+    auto* rc = static_cast<RefCircuit*>(h);
+    Circuit& c = *rc->c;
+    std::vector<size_t> qs;
+    for (unsigned i = 0; i < rc->n; ++i) qs.push_back(i);
+    switch (which) {
+    case 0: c.pauliX(0); QFT::createQFT(c, qs); return 0;
+    case 1: c.pauliX(0); QFT::createIQFT(c, qs); return 0;
+    case 2: Grover::createGroverCircuit(c, int(rc->n), target, iterations); return 0;
+    default: return -1;
+    }
+#else
+    (void)h; (void)which; (void)target; (void)iterations;
+    return -1;
+#endif
 }
 
 uint64_t ref_circuit_measure(void* h)

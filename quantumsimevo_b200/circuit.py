@@ -228,15 +228,37 @@ class Circuit:
         self._push(L.make_op(L.SWAP, self._q(q0), self._q(q1)), f"SWAP (q0: {q0}, q1: {q1})")
 
     def add_ops(self, ops) -> None:
-        """Queue an OP_DTYPE array (or op tuples) at once."""
-        arr = L.as_ops(ops)
-        for o in arr:
-            self._ops.append(tuple(o.tolist()))
-            self._desc.append(L.GATE_NAMES.get(int(o["type"]), "?"))
+        """Queue an OP_DTYPE array (or op tuples) at once.  The array is kept as one
+        entry of the queue (no per-gate Python objects, so long circuits queue fast)."""
+        arr = L.as_ops(ops).copy()
+        if len(arr):
+            self._ops.append(arr)
+            self._desc.append(arr)
 
     @property
     def ops(self) -> np.ndarray:
-        return L.as_ops(self._ops)
+        parts, run = [], []
+        for o in self._ops:
+            if isinstance(o, np.ndarray):
+                if run:
+                    parts.append(L.as_ops(run))
+                    run = []
+                parts.append(o)
+            else:
+                run.append(o)
+        if run:
+            parts.append(L.as_ops(run))
+        if not parts:
+            return L.as_ops([])
+        return parts[0] if len(parts) == 1 else np.concatenate(parts)
+
+    def _descriptions(self):
+        for d in self._desc:
+            if isinstance(d, np.ndarray):
+                for o in d:
+                    yield L.GATE_NAMES.get(int(o["type"]), "?")
+            else:
+                yield d
 
     # ---- execution & measurement ----
     def execute(self, print_steps: bool = False, noise_uniforms=None, params=None):
@@ -246,7 +268,7 @@ class Circuit:
         values of the parameters that queued gates reference (param=k)."""
         if print_steps:
             print("Initial state: |0...0>")
-            for d in self._desc:
+            for d in self._descriptions():
                 print("Executing:", d)
         ops = self.ops
         stats = L.QseExecStats()

@@ -307,6 +307,7 @@ void execute_program(qse_state* st, const qse_op* ops, size_t nops, const double
         opt.k = tile_qubits_for(ctx, st->n, 4, 12);
         opt.max_gates = uint32_t(std::max(0, ctx->max_gates_per_pass));
         if (ctx->jit && (opt.max_gates == 0 || opt.max_gates > plan::kJitMaxGates)) opt.max_gates = plan::kJitMaxGates;
+        opt.zz_fuse = true;
         bool use_jit = false;
         std::vector<jit::Source> srcs;
         plan::Plan pl = plan_for(st, gates, opt, 1, use_jit, srcs);

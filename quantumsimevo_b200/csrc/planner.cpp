@@ -557,9 +557,46 @@ private:
 
 }  // namespace
 
-Plan build(const std::vector<Gate>& gates, uint32_t n, const uint32_t* perm_in, const Options& opt)
+// CNOT(c,t) RZ(th,t) CNOT(c,t) multiplies |c t> by e^{-i th/2} e^{i th (c XOR t)}, and
+// c XOR t = c + t - 2ct: the diagonal RZ(th,c) PHASE(th,t) CPHASE(-2th,c,t), global
+// phase included.  QAOA cost layers written with CNOTs (QSEplayground/QAOA.cpp:128-133)
+// then need no pass of their own.  Returns false when nothing matched.
+static bool fuse_zz(const std::vector<Gate>& gates, std::vector<Gate>& out)
+{
+    bool any = false;
+    for (size_t i = 0; i + 2 < gates.size(); ++i) {
+        const Gate& a = gates[i];
+        const Gate& b = gates[i + 1];
+        const Gate& c = gates[i + 2];
+        if (a.type != QSE_GATE_CNOT || b.type != QSE_GATE_RZ || c.type != QSE_GATE_CNOT) continue;
+        if (a.c != c.c || a.t != c.t || b.t != a.t || a.c == a.t) continue;
+        if (a.grad >= 0 || b.grad >= 0 || c.grad >= 0) continue;
+        if (!any) out = gates;
+        any = true;
+        Gate rz = b;
+        rz.t = a.c;
+        Gate ph{};
+        ph.type = QSE_GATE_PHASE;
+        ph.t = a.t;
+        ph.theta = b.theta;
+        Gate cp{};
+        cp.type = QSE_GATE_CPHASE;
+        cp.t = a.t;
+        cp.c = a.c;
+        cp.theta = -2.0 * b.theta;
+        out[i] = rz;
+        out[i + 1] = ph;
+        out[i + 2] = cp;
+        i += 2;
+    }
+    return any;
+}
+
+Plan build(const std::vector<Gate>& gates_in, uint32_t n, const uint32_t* perm_in, const Options& opt)
 {
     if (n == 0 || n > 40) fail(QSE_ERR_SIZE, "planner: unsupported qubit count");
+    std::vector<Gate> fused;
+    const std::vector<Gate>& gates = (opt.zz_fuse && fuse_zz(gates_in, fused)) ? fused : gates_in;
     Plan plan;
     uint32_t perm[64];
     for (uint32_t q = 0; q < 64; ++q) perm[q] = q < n ? perm_in[q] : q;
@@ -585,7 +622,9 @@ Plan build(const std::vector<Gate>& gates, uint32_t n, const uint32_t* perm_in, 
         std::vector<size_t> deferred;
         uint32_t nN = 0, nterms = 0, nslots = 0;
         double gph = 0.0;
-        for (size_t idx : remaining) {
+        const uint64_t allq = n >= 64 ? ~uint64_t(0) : (bit(n) - 1);
+        for (size_t r = 0; r < remaining.size(); ++r) {
+            const size_t idx = remaining[r];
             const Info& in = info[idx];
             const Gate& g = gates[idx];
             bool blocked = ((in.nset | in.dset) & bN) || (in.nset & bD);
@@ -623,6 +662,12 @@ Plan build(const std::vector<Gate>& gates, uint32_t n, const uint32_t* perm_in, 
             deferred.push_back(idx);
             bN |= in.nset;
             bD |= in.dset;
+            if ((bN & allq) == allq) {
+                // every later gate shares a qubit with a deferred non-diagonal one:
+                // none can join this pass (keeps planning linear in the gate count)
+                deferred.insert(deferred.end(), remaining.begin() + r + 1, remaining.end());
+                break;
+            }
         }
         // fill the tile with the lowest unused physical qubits
         for (uint32_t q = 0; q < n && uint32_t(popc(T)) < k; ++q) T |= bit(q);

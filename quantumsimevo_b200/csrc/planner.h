@@ -138,6 +138,9 @@ struct Options {
     bool acc_mul = false;        // accumulator groups (K_ACC_THR / K_ACC_REG) are direct too:
                                  // kernels multiply their (cos, sin) into per-thread complex
                                  // factors instead of summing angles and calling sincos per flush
+    bool zz_fuse = false;        // rewrite CNOT(c,t) RZ(th,t) CNOT(c,t) as the diagonal
+                                 // RZ(th,c) PHASE(th,t) CPHASE(-2th,c,t) (same three slots;
+                                 // only for plans whose angles are never rebound)
     bool keep_gphase = true;     // false: drop RZ's global phase (expectations and gradients
                                  // do not see it; the pass programs then depend on angles
                                  // only through op_angles / term_angles)

@@ -207,12 +207,26 @@ def load_reference(gpu=False):
         "ref_statevector_set": ([_vp, _vp], None),
         "ref_statevector_measure_qubit": ([_vp, C.c_uint], C.c_int),
         "ref_statevector_reset_qubit": ([_vp, C.c_uint], None),
+        "ref_playground_build": ([_vp, C.c_int, C.c_int, C.c_int], C.c_int),
     }
     for name, (a, r) in sigs.items():
         f = getattr(lib, name)
         f.argtypes = a
         f.restype = r
     return lib
+
+
+def ref_playground(ref, which, n, target=0, iterations=0):
+    """State from the reference playground's own builder (0 = runQFT's circuit, 1 = runIQFT's,
+    2 = Grover::createGroverCircuit) on the reference Circuit with the scalar backend."""
+    assert ref.ref_set_backend(0) == 0
+    h = ref.ref_circuit_new(n, 0)
+    assert ref.ref_playground_build(h, which, target, iterations) == 0
+    ref.ref_circuit_execute(h, 0)
+    out = np.empty(1 << n, dtype=np.complex128)
+    ref.ref_circuit_state(h, out.ctypes.data_as(_vp))
+    ref.ref_circuit_free(h)
+    return out
 
 
 def ref_run(ref, n, ops, backend=0):
