@@ -487,9 +487,9 @@ __global__ void __launch_bounds__(kBT) k_prob_identity(const double2* __restrict
 // img[b] = 2^b with a host-chosen low nibble for b >= 4, so that both the
 // write side (lanes vary r's bits 0..4) and the read side (lanes vary the
 // read-order images of logical bits 0..4) touch 16 distinct 8-byte bank pairs
-// per half-warp.  Each warp's 32 written probabilities share one 4096-block of
-// the logical array; their sum goes to that block's approximate sum (atomic:
-// only the binade guess reads it).
+// per half-warp.  Each warp's 32 written probabilities of one j share one
+// 4096-block of the logical array; their sum goes to that block's approximate
+// sum (atomic: only the binade guess reads it).
 struct GatherPlan {
     uint64_t outer_mask;      // physical bits outside S
     uint8_t sphys[12];        // S ascending (tile order for the reads)
@@ -540,6 +540,7 @@ __global__ void __launch_bounds__(kBT) k_prob_gather(const double2* __restrict__
         sm[sw ^ so] = norm2(amp[tr | off]);
     }
     __syncthreads();
+    double ws[kEPT];
 #pragma unroll
     for (int j = 0; j < kEPT; ++j) {
         uint64_t off = 0;
@@ -552,9 +553,31 @@ __global__ void __launch_bounds__(kBT) k_prob_gather(const double2* __restrict__
             }
         const double v = sm[sr ^ so];
         prob[tw | off] = v;
-        double ws = v;
-        for (int o = 16; o > 0; o >>= 1) ws += __shfl_xor_sync(0xffffffffu, ws, o);
-        if ((t & 31) == 0) atomicAdd(bsum + ((tw | off) >> 12), ws);
+        ws[j] = v;
+    }
+    // Warp sums of the 16 values (one 4096-block per j): a transpose-reduce
+    // butterfly.  Each step trades half of a lane's remaining partial sums with
+    // the partner lane and keeps the half its lane bit selects, so after four
+    // steps lane l holds the 16-lane sum for j = (l >> 1) & 15 and the last
+    // exchange completes it (32 shuffles per lane instead of 160).
+    const uint32_t lane = t & 31;
+#pragma unroll
+    for (int h = 8, lb = 16; h >= 1; h >>= 1, lb >>= 1) {
+        const bool up = (lane & uint32_t(lb)) != 0;
+#pragma unroll
+        for (int k = 0; k < h; ++k) {
+            const double lo = ws[k], hi = ws[k + h];
+            const double give = up ? lo : hi;
+            ws[k] = (up ? hi : lo) + __shfl_xor_sync(0xffffffffu, give, lb);
+        }
+    }
+    ws[0] += __shfl_xor_sync(0xffffffffu, ws[0], 1);
+    if ((lane & 1) == 0) {
+        const uint32_t j = (lane >> 1) & 15;
+        uint64_t off = 0;
+        for (int b = 0; b < 4; ++b)
+            if ((j >> b) & 1) off |= uint64_t(1) << g.slog[8 + b];
+        atomicAdd(bsum + ((tw | off) >> 12), ws[0]);
     }
 }
 
