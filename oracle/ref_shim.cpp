@@ -40,6 +40,7 @@
 #define private public
 #include "Grover.h"
 #undef private
+#include "TVS.h"
 #endif
 
 static int g_backend = 0;
@@ -187,6 +188,36 @@ int ref_playground_build(void* h, int which, int target, int iterations)
     }
 #else
     (void)h; (void)which; (void)target; (void)iterations;
+    return -1;
+#endif
+}
+
+// TVS::buildIsing (TVS.cpp:31-99) on an n x n distance matrix (row-major):
+// fields into h (n*n), couplings into pairs (2 per coupling, i < j) and coeffs
+// in the reference's hash-map order; *npairs receives their count (at most cap).
+// Returns -1 without the playground sources or when cap is too small.
+int ref_tsp_ising(const double* dist, unsigned n, double penalty, double weight, int row_constraint,
+                  int col_constraint, double* h, unsigned* pairs, double* coeffs, unsigned cap, unsigned* npairs)
+{
+#ifdef QSE_REF_WITH_PLAYGROUND
+    std::vector<std::vector<double>> d(n, std::vector<double>(n));
+    for (unsigned a = 0; a < n; ++a)
+        for (unsigned b = 0; b < n; ++b) d[a][b] = dist[a * n + b];
+    std::vector<std::pair<size_t, size_t>> zz;
+    std::vector<double> c;
+    std::vector<double> hv = TVS::buildIsing(n, penalty, weight, d, zz, c, row_constraint != 0, col_constraint != 0);
+    if (zz.size() > cap) return -1;
+    for (size_t i = 0; i < hv.size(); ++i) h[i] = hv[i];
+    for (size_t k = 0; k < zz.size(); ++k) {
+        pairs[2 * k] = unsigned(zz[k].first);
+        pairs[2 * k + 1] = unsigned(zz[k].second);
+        coeffs[k] = c[k];
+    }
+    *npairs = unsigned(zz.size());
+    return 0;
+#else
+    (void)dist; (void)n; (void)penalty; (void)weight; (void)row_constraint; (void)col_constraint;
+    (void)h; (void)pairs; (void)coeffs; (void)cap; (void)npairs;
     return -1;
 #endif
 }

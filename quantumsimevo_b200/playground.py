@@ -109,6 +109,105 @@ def maxcut30(p: int = 3) -> np.ndarray:
     return qaoa_maxcut(30, MAXCUT30_EDGES, [math.pi / 8] * p, [math.pi / 3] * p)
 
 
+# tsp() (QSEplayground.cpp:16-45): 5 cities -> 25 qubits; TVS::runTVS(dist5, -1, 1, 0.8, 0.4, 100000)
+TSP5_DIST = [[0, 3, 4, 2, 7], [3, 0, 5, 7, 6], [4, 5, 0, 6, 3], [2, 7, 6, 0, 5], [7, 6, 3, 5, 0]]
+
+
+def tsp_index(city: int, step: int, n: int) -> int:
+    """TVS::getIndex (TVS.cpp:10-13): qubit of "city at step"."""
+    return city * n + step
+
+
+def tsp_ising(n, penalty, weight, dist, row_constraint=True, col_constraint=True):
+    """TVS::buildIsing (TVS.cpp:31-99): the TSP QUBO in Ising form, fields h and couplings
+    J (pairs i < j), accumulated in the reference's order so every coefficient is the same
+    double.  Returns (h, pairs, coeffs) with pairs in first-insertion order."""
+    qubits = n * n
+    h = [0.0] * qubits
+    J = {}
+
+    def add_zz(a, b, c):
+        if a > b:
+            a, b = b, a
+        J[(a, b)] = J.get((a, b), 0.0) + c
+
+    def add_linear(i, c):
+        h[i] -= c / 2.0
+
+    def add_quad(i, j, q):
+        h[i] -= q / 4.0
+        h[j] -= q / 4.0
+        add_zz(i, j, q / 4.0)
+
+    def add_constraint(group):
+        for a in range(len(group)):
+            add_linear(group[a], -penalty)
+            for b in range(a + 1, len(group)):
+                add_quad(group[a], group[b], 2.0 * penalty)
+
+    if row_constraint:
+        for v in range(n):
+            add_constraint([tsp_index(v, t, n) for t in range(n)])
+    if col_constraint:
+        for t in range(n):
+            add_constraint([tsp_index(v, t, n) for v in range(n)])
+    for u in range(n):
+        for v in range(n):
+            if u == v:
+                continue
+            q = weight * dist[u][v]
+            for t in range(n):
+                add_quad(tsp_index(u, t, n), tsp_index(v, (t + 1) % n, n), q)
+    pairs = [k for k, c in J.items() if abs(c) >= 1e-15]
+    return h, pairs, [J[k] for k in pairs]
+
+
+def tsp_schedule(penalty, weight, gamma, beta, layers, dist):
+    """TVS::runTVS (TVS.cpp:292-308): the automatic penalty (negative -> weight * maxDist * n
+    + 1) and the per-layer ramps gamma_k = gamma (k+1)/p, beta_k = beta (1 - (k+1)/p) + beta/4."""
+    n = len(dist)
+    if penalty < 0.0:
+        penalty = weight * max(max(r) for r in dist) * float(n) + 1.0
+    layers = max(layers, 1)
+    gammas, betas = [], []
+    for k in range(layers):
+        frac = 1.0 if layers == 1 else (k + 1) / layers
+        gammas.append(gamma * frac)
+        betas.append(beta * (1.0 - frac) + beta * 0.25)
+    return penalty, gammas, betas
+
+
+def tsp_xy_qaoa(dist, penalty, weight, gammas, betas) -> np.ndarray:
+    """TVS::createCircuit (TVS.cpp:118-179): X on the identity tour, then per layer the
+    ZZ phases CNOT RZ(2 gamma J) CNOT and RZ(2 gamma h) on every qubit (column penalty and
+    route cost; the row constraint is left to the mixer), then the XY ring mixer inside
+    each city row, each pair as Rxx(2 beta) (H-conjugated CNOT RZ CNOT) then Ryy(2 beta)
+    (RX(+-pi/2)-conjugated).  The reference emits the ZZ pairs in its hash map's order;
+    they commute, so any fixed order gives the same state up to rounding."""
+    n = len(dist)
+    qubits = n * n
+    h, pairs, coeffs = tsp_ising(n, penalty, weight, dist, row_constraint=False, col_constraint=True)
+    ops = [_op(X, tsp_index(v, v, n)) for v in range(n)]
+    for gamma, beta in zip(gammas, betas):
+        for (q1, q2), c in zip(pairs, coeffs):
+            ops += [_op(CNOT, q2, q1), _op(RZ, q2, theta=2 * gamma * c), _op(CNOT, q2, q1)]
+        ops += [_op(RZ, q, theta=2 * gamma * h[q]) for q in range(qubits)]
+        for v in range(n):
+            for t in range(n):
+                a, b = tsp_index(v, t, n), tsp_index(v, (t + 1) % n, n)
+                ops += [_op(H, a), _op(H, b), _op(CNOT, b, a), _op(RZ, b, theta=2 * beta), _op(CNOT, b, a),
+                        _op(H, a), _op(H, b),
+                        _op(RX, a, theta=PI / 2), _op(RX, b, theta=PI / 2),
+                        _op(CNOT, b, a), _op(RZ, b, theta=2 * beta), _op(CNOT, b, a),
+                        _op(RX, a, theta=-PI / 2), _op(RX, b, theta=-PI / 2)]
+    return to_array(ops)
+
+
+def tsp5() -> np.ndarray:
+    penalty, gammas, betas = tsp_schedule(-1.0, 1.0, 0.8, 0.4, 4, TSP5_DIST)
+    return tsp_xy_qaoa(TSP5_DIST, penalty, 1.0, gammas, betas)
+
+
 @dataclass
 class Workload:
     name: str
@@ -135,4 +234,5 @@ def workloads() -> list:
         Workload("iqft30", 30, 1000, lambda: iqft(30), 125000.0, "AVX2 CPU"),
         Workload("grover25", grover_size(gt)[0], 10000, lambda: grover(gt), 4950000.0, "CUDA"),
         Workload("maxcut30_p3", 30, 1500000, lambda: maxcut30(3), 278000.0, "CPU (30 q exceeds 8 GB)"),
+        Workload("tsp5_p4", 25, 100000, tsp5, 12000.0, "CUDA"),
     ]

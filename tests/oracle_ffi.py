@@ -208,6 +208,8 @@ def load_reference(gpu=False):
         "ref_statevector_measure_qubit": ([_vp, C.c_uint], C.c_int),
         "ref_statevector_reset_qubit": ([_vp, C.c_uint], None),
         "ref_playground_build": ([_vp, C.c_int, C.c_int, C.c_int], C.c_int),
+        "ref_tsp_ising": ([_pd, C.c_uint, _d, _d, C.c_int, C.c_int, _pd, C.POINTER(C.c_uint), _pd, C.c_uint,
+                           C.POINTER(C.c_uint)], C.c_int),
     }
     for name, (a, r) in sigs.items():
         f = getattr(lib, name)

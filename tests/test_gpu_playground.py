@@ -27,6 +27,15 @@ def _run(dev, n, ops, shots=3000, seed=0):
     return st
 
 
+# tsp(): the 4-city distances of QSEplayground.cpp, two layers of the XY-mixer ansatz
+_DIST4 = [[0, 3, 4, 2], [3, 0, 5, 7], [4, 5, 0, 6], [2, 7, 6, 0]]
+
+
+def _tsp4_schedule():
+    penalty, gammas, betas = P.tsp_schedule(-1.0, 1.0, 0.8, 0.4, 2, _DIST4)
+    return penalty, 1.0, gammas, betas
+
+
 CASES = [
     ("ghz", 16, lambda: P.ghz(16)),
     ("qft", 14, lambda: P.qft(14)),
@@ -37,6 +46,7 @@ CASES = [
     ("grover", 13, lambda: P.grover(5000)),
     ("maxcut", 14, lambda: P.qaoa_maxcut(14, [(i, (i + 1) % 14) for i in range(14)] +
                                          [(i, i + 7) for i in range(7)], [0.39, 0.81, 0.2], [1.05, 0.3, 0.7])),
+    ("tsp", 16, lambda: P.tsp_xy_qaoa(_DIST4, *_tsp4_schedule())),
 ]
 
 

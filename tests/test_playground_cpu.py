@@ -89,3 +89,48 @@ def test_grover_plan_is_linear_in_iterations():
     # planning stops scanning once every qubit is blocked: passes grow linearly
     a, b, c = (_passes(P.grover(29123321, iterations=it), 25) for it in (10, 20, 30))
     assert b - a == c - b > 0
+
+
+def _ref_ising(ref, dist, penalty, weight, row, col):
+    n = len(dist)
+    d = np.ascontiguousarray(np.asarray(dist, dtype=np.float64).reshape(-1))
+    h = np.zeros(n * n)
+    cap = (n * n) ** 2
+    pairs = (C.c_uint * (2 * cap))()
+    coeffs = np.zeros(cap)
+    cnt = C.c_uint()
+    assert ref.ref_tsp_ising(d.ctypes.data_as(O._pd), n, penalty, weight, int(row), int(col),
+                             h.ctypes.data_as(O._pd), pairs, coeffs.ctypes.data_as(O._pd), cap, C.byref(cnt)) == 0
+    return h, {(pairs[2 * k], pairs[2 * k + 1]): coeffs[k] for k in range(cnt.value)}
+
+
+@pytest.mark.parametrize("row,col", [(False, True), (True, True)])
+def test_tsp_ising_matches_reference(ref, row, col):
+    # the reference's own TVS::buildIsing: every field and coupling the same double
+    penalty, _, _ = P.tsp_schedule(-1.0, 1.0, 0.8, 0.4, 4, P.TSP5_DIST)
+    assert penalty == 36.0
+    h_ref, j_ref = _ref_ising(ref, P.TSP5_DIST, penalty, 1.0, row, col)
+    h, pairs, coeffs = P.tsp_ising(5, penalty, 1.0, P.TSP5_DIST, row, col)
+    assert np.array_equal(np.array(h), h_ref)
+    assert dict(zip(pairs, coeffs)) == j_ref
+
+
+def test_tsp_circuit_stays_in_the_feasible_rows(ref):
+    # 3 cities (9 qubits): the XY ring mixer keeps one excitation per city row
+    dist = [[0, 2, 5], [2, 0, 3], [5, 3, 0]]
+    penalty, gammas, betas = P.tsp_schedule(-1.0, 1.0, 0.8, 0.4, 2, dist)
+    ops = P.tsp_xy_qaoa(dist, penalty, 1.0, gammas, betas)
+    st = O.run(9, ops)
+    assert np.max(np.abs(st - O.ref_run(ref, 9, ops))) <= 1e-12
+    idx = np.arange(1 << 9)
+    rows_ok = np.ones(1 << 9, dtype=bool)
+    for v in range(3):
+        w = sum(((idx >> P.tsp_index(v, t, 3)) & 1) for t in range(3))
+        rows_ok &= w == 1
+    assert abs(np.sum(np.abs(st[rows_ok]) ** 2) - 1.0) <= 1e-12
+
+
+def test_tsp5_workload_shape():
+    ops = P.tsp5()
+    _, pairs, _ = P.tsp_ising(5, 36.0, 1.0, P.TSP5_DIST, False, True)
+    assert len(ops) == 5 + 4 * (3 * len(pairs) + 25 + 25 * 14)
