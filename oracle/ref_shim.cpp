@@ -275,6 +275,35 @@ void* ref_backend_new(int b)
 
 void ref_backend_free(void* be) { delete static_cast<ICircuitUnitaryOperation*>(be); }
 
+// CircuitUnitaryOperationB200's sample / measure extensions on a backend made
+// by ref_backend_new(3) (only in libqse_ref_gpu.so); -1 for another backend.
+int ref_b200_sample(void* be, void* svp, const double* u, size_t shots, uint64_t* out)
+{
+#ifdef QSE_REF_WITH_GPU
+    auto* b = dynamic_cast<CircuitUnitaryOperationB200*>(static_cast<ICircuitUnitaryOperation*>(be));
+    if (!b) return -1;
+    std::vector<size_t> r = b->sample(*static_cast<StateVector*>(svp), u, shots);
+    for (size_t i = 0; i < r.size(); ++i) out[i] = r[i];
+    return 0;
+#else
+    (void)be; (void)svp; (void)u; (void)shots; (void)out;
+    return -1;
+#endif
+}
+
+int ref_b200_measure(void* be, void* svp, double u, uint64_t* out)
+{
+#ifdef QSE_REF_WITH_GPU
+    auto* b = dynamic_cast<CircuitUnitaryOperationB200*>(static_cast<ICircuitUnitaryOperation*>(be));
+    if (!b) return -1;
+    *out = b->measure(*static_cast<StateVector*>(svp), u);
+    return 0;
+#else
+    (void)be; (void)svp; (void)u; (void)out;
+    return -1;
+#endif
+}
+
 void* ref_statevector_new(unsigned n) { Quiet q(true); return new StateVector(n); }
 void ref_statevector_free(void* sv) { delete static_cast<StateVector*>(sv); }
 

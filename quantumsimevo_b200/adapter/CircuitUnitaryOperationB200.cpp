@@ -167,3 +167,19 @@ void CircuitUnitaryOperationB200::executeProgram(StateVector& sv, const std::vec
     qse_exec_stats stats{};
     QSE_TIMED("Program", qse_execute(state_, ops.data(), ops.size(), nullptr, 0, nullptr, nullptr, 0, &stats));
 }
+
+std::vector<size_t> CircuitUnitaryOperationB200::sample(StateVector& sv, const double* uniforms, size_t shots)
+{
+    ensureOnDevice(sv);
+    std::vector<uint64_t> out(shots);
+    if (shots) check(qse_sample(state_, uniforms, shots, 0, out.data()), "qse_sample");
+    return std::vector<size_t>(out.begin(), out.end());
+}
+
+size_t CircuitUnitaryOperationB200::measure(StateVector& sv, double u)
+{
+    ensureOnDevice(sv);
+    uint64_t idx = 0;
+    check(qse_measure(state_, u, &idx), "qse_measure");
+    return static_cast<size_t>(idx);
+}

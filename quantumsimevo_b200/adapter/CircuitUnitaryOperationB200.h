@@ -45,6 +45,16 @@ public:
     // (the fusion planner path): one call, any number of passes.
     void executeProgram(StateVector& sv, const std::vector<GateCommand>& commands);
 
+    // Extensions for Circuit::sample / Circuit::measure (StateVector.cpp:77-156)
+    // on the device copy, so neither needs the full-state copy to the host.
+    // Each shot / the measurement takes its uniform draw u in [0, 1) from the
+    // caller (the reference draws from std::random_device); the outcome is the
+    // one StateVector::sample / measure gives for the same draw.  measure()
+    // collapses the device copy, which stays authoritative (flush() brings it
+    // to the host).
+    std::vector<size_t> sample(StateVector& sv, const double* uniforms, size_t shots);
+    size_t measure(StateVector& sv, double u);
+
 private:
     void ensureOnDevice(StateVector& sv);
     void check(int status, const char* what) const;

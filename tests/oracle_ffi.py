@@ -211,6 +211,9 @@ def load_reference(gpu=False):
         "ref_tsp_ising": ([_pd, C.c_uint, _d, _d, C.c_int, C.c_int, _pd, C.POINTER(C.c_uint), _pd, C.c_uint,
                            C.POINTER(C.c_uint)], C.c_int),
     }
+    if gpu:
+        sigs["ref_b200_sample"] = ([_vp, _vp, _pd, _sz, _pu64], C.c_int)
+        sigs["ref_b200_measure"] = ([_vp, _vp, _d, _pu64], C.c_int)
     for name, (a, r) in sigs.items():
         f = getattr(lib, name)
         f.argtypes = a

@@ -88,6 +88,33 @@ def test_adapter_flush_and_host_dirty(ref):
     ref.ref_backend_free(be)
 
 
+def test_adapter_sample_and_measure_extensions(ref):
+    # CircuitUnitaryOperationB200::sample / measure with injected uniforms: the
+    # outcomes StateVector::sample / measure give for the same draws, and the
+    # collapse lands on the host at the next flush
+    n = 12
+    be = ref.ref_backend_new(3)
+    sv = ref.ref_statevector_new(n)
+    ops = np.ascontiguousarray(W.random_circuit(n, 150, 85, with_2x2=True))
+    assert ref.ref_backend_apply(be, sv, ops.ctypes.data_as(C.c_void_p), len(ops)) == 0
+    ref.ref_backend_flush(be)
+    st = np.empty(1 << n, dtype=np.complex128)
+    ref.ref_statevector_get(sv, st.ctypes.data_as(C.c_void_p))
+    u = np.random.default_rng(85).random(3000)
+    out = np.empty(len(u), dtype=np.uint64)
+    assert ref.ref_b200_sample(be, sv, u.ctypes.data_as(O._pd), len(u), out.ctypes.data_as(O._pu64)) == 0
+    assert np.array_equal(out, O.sample(st, n, u))
+    idx = np.zeros(1, dtype=np.uint64)
+    assert ref.ref_b200_measure(be, sv, 0.437, idx.ctypes.data_as(O._pu64)) == 0
+    want_idx, want_st = O.measure(st, n, 0.437)
+    assert int(idx[0]) == want_idx
+    ref.ref_backend_flush(be)
+    ref.ref_statevector_get(sv, st.ctypes.data_as(C.c_void_p))
+    assert np.array_equal(st, want_st)
+    ref.ref_statevector_free(sv)
+    ref.ref_backend_free(be)
+
+
 def test_torch_autograd_matches_oracle_and_fd():
     n = 10
     ops, params, edges, obs_t = W.qaoa_maxcut(n, 2, seed=90)
