@@ -614,7 +614,9 @@ Plan build(const std::vector<Gate>& gates_in, uint32_t n, const uint32_t* perm_i
     // scale each pass, their K_GRAD_* weights assume it
     std::pair<double, double> carry{1.0, 0.0};
 
-    while (!remaining.empty()) {
+    // remaining[head..) are the gates still to plan, in order
+    size_t head = 0;
+    while (head < remaining.size()) {
         uint64_t T = 0;
         for (uint32_t q = 0; q < seed_bits; ++q) T |= bit(q);
         uint64_t bN = 0, bD = 0;
@@ -623,7 +625,8 @@ Plan build(const std::vector<Gate>& gates_in, uint32_t n, const uint32_t* perm_i
         uint32_t nN = 0, nterms = 0, nslots = 0;
         double gph = 0.0;
         const uint64_t allq = n >= 64 ? ~uint64_t(0) : (bit(n) - 1);
-        for (size_t r = 0; r < remaining.size(); ++r) {
+        size_t stop = remaining.size();   // first gate this pass did not look at
+        for (size_t r = head; r < remaining.size(); ++r) {
             const size_t idx = remaining[r];
             const Info& in = info[idx];
             const Gate& g = gates[idx];
@@ -665,7 +668,7 @@ Plan build(const std::vector<Gate>& gates_in, uint32_t n, const uint32_t* perm_i
             if ((bN & allq) == allq) {
                 // every later gate shares a qubit with a deferred non-diagonal one:
                 // none can join this pass (keeps planning linear in the gate count)
-                deferred.insert(deferred.end(), remaining.begin() + r + 1, remaining.end());
+                stop = r + 1;
                 break;
             }
         }
@@ -682,9 +685,13 @@ Plan build(const std::vector<Gate>& gates_in, uint32_t n, const uint32_t* perm_i
         prog.outer_mask = all & ~T;
         prog.ngates = uint32_t(abs.size());
         Lowering low(prog, n, opt);
-        carry = low.run(abs, gph, carry, opt.grads || deferred.empty());
+        const bool last = deferred.empty() && stop == remaining.size();
+        carry = low.run(abs, gph, carry, opt.grads || last);
         plan.passes.push_back(std::move(prog));
-        remaining.swap(deferred);
+        // next: this pass's deferred gates, then the ones it did not look at
+        // (written in place just before those, no copy of the unscanned rest)
+        head = stop - deferred.size();
+        std::copy(deferred.begin(), deferred.end(), remaining.begin() + std::ptrdiff_t(head));
     }
     for (uint32_t q = 0; q < 64; ++q) plan.perm_final[q] = perm[q];
     return plan;
