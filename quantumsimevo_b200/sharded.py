@@ -9,7 +9,9 @@ global.  Gates lower per rank (``lower``):
   gate, a per-rank scalar, or nothing;
 - a CNOT whose control is global becomes X on its target on the ranks whose
   control bit is 1;
-- SWAP only relabels (as in the single-state engine);
+- SWAP only relabels (as in the single-state engine), and so do X and Y on a
+  global qubit (they flip which ranks hold its 0 and 1; Y adds a per-rank
+  phase); a relabelling left at the end is resolved by one exchange;
 - a non-diagonal gate on a global qubit first exchanges that qubit with a
   local one: each rank trades the half of its shard whose local bit differs
   from its global bit with the partner rank that differs in that global bit
@@ -63,6 +65,7 @@ def lower(ops, n: int, g: int, rank: int, params=None):
         raise ValueError("need at least one local qubit")
     pos = list(range(n))
     where = list(range(n))
+    flip = [0] * g          # X on a global qubit relabels: its value on rank r is bit j of r XOR flip[j]
     steps, pending = [], []
     scalar = [1.0 + 0.0j]
 
@@ -80,14 +83,35 @@ def lower(ops, n: int, g: int, rank: int, params=None):
 
     def gbit(q):
         p = pos[q]
-        return None if p < nl else (rank >> (p - nl)) & 1
+        return None if p < nl else ((rank >> (p - nl)) & 1) ^ flip[p - nl]
 
-    def next_use(i, q):
-        for k in range(i, len(ops)):
-            t = int(ops[k]["type"])
-            if (t in _NONDIAG or t == L.CNOT) and int(ops[k]["target"]) == q:
-                return k
-        return len(ops) + 1
+    def exchange(j, lp):
+        # global position nl + j <-> local position lp; a flipped global qubit
+        # arrives holding the rank's bit, so one local X restores its value
+        flush_scalar()
+        flush_ops()
+        steps.append(("exchange", j, lp))
+        qg, ql = where[nl + j], where[lp]
+        pos[qg], pos[ql] = lp, nl + j
+        where[lp], where[nl + j] = qg, ql
+        if flip[j]:
+            pending.append(_mk(L.X, lp))
+            flip[j] = 0
+
+    types = ops["type"].astype(np.int64)
+    targets = ops["target"].astype(np.int64)
+    nondiag = np.isin(types, list(_NONDIAG) + [L.CNOT])
+
+    def next_uses(i):
+        # index of each qubit's next non-diagonal use at or after op i (one scan)
+        nu = {}
+        for k in np.nonzero(nondiag[i:])[0]:
+            q = int(targets[i + k])
+            if q not in nu:
+                nu[q] = i + int(k)
+                if len(nu) == n:
+                    break
+        return nu
 
     for i, op in enumerate(ops):
         t = int(op["type"])
@@ -99,16 +123,18 @@ def lower(ops, n: int, g: int, rank: int, params=None):
             pos[a], pos[b] = pos[b], pos[a]
             where[pos[a]], where[pos[b]] = a, b
             continue
+        if t in (L.X, L.Y) and pos[tq] >= nl:
+            # X and Y on a global qubit move no data: flip which ranks hold 0 and 1
+            j = pos[tq] - nl
+            flip[j] ^= 1
+            if t == L.Y:                  # Y|v> = i (-1)^v |1-v>: a phase by the new value
+                scalar[0] *= 1j if gbit(tq) == 1 else -1j
+            continue
         if t in _NONDIAG or t == L.CNOT:
             if pos[tq] >= nl:
-                flush_scalar()
-                flush_ops()
-                best = max(range(nl), key=lambda lp: (next_use(i, where[lp]), lp))
-                j = pos[tq] - nl
-                steps.append(("exchange", j, best))
-                ql = where[best]
-                pos[tq], pos[ql] = best, nl + j
-                where[best], where[nl + j] = tq, ql
+                nu = next_uses(i)
+                best = max(range(nl), key=lambda lp: (nu.get(where[lp], len(ops) + 1), lp))
+                exchange(pos[tq] - nl, best)
             if t == L.CNOT:
                 cv = gbit(int(op["control"]))
                 if cv is None:
@@ -153,6 +179,9 @@ def lower(ops, n: int, g: int, rank: int, params=None):
             for p in loc[:-1]:
                 mask |= 1 << p
             pending.append(_mk(L.MCPHASE, loc[-1], 0, theta=th, controls=mask))
+    for j in range(g):
+        if flip[j]:                       # leave no relabelling behind: the shards hold the state
+            exchange(j, nl - 1)
     flush_scalar()
     flush_ops()
     return steps, pos

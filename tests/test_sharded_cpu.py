@@ -1,6 +1,7 @@
 """One state sharded over ranks (quantumsimevo_b200/sharded.py) on CPU: the
-lowering, the half-shard exchanges and the final qubit map, with the FP64 oracle
-as every shard's local executor.  All shards in one process (LocalTransport) for
+lowering (including X and Y on global qubits as relabellings), the half-shard
+exchanges and the final qubit map, with the FP64 oracle as every shard's local
+executor.  All shards in one process (LocalTransport) for
 2, 4 and 8 ranks, and two gloo ranks in two processes (TorchDistTransport)."""
 import math
 import os
@@ -32,7 +33,9 @@ def _mixed(n, seed):
         extra += [_op(L.CNOT, int(a), int(b)), _op(L.RZ, int(a), theta=th), _op(L.CNOT, int(a), int(b)),
                   _op(L.MCPHASE, int(c), 0, th, (1 << int(a)) | (1 << int(b))),
                   _op(L.CPHASE, int(b), int(c), th), _op(L.Z, int(c)), _op(L.PHASE, int(a), theta=th),
-                  _op(L.SWAP, int(a), int(c)), _op(L.H, int(b))]
+                  _op(L.SWAP, int(a), int(c)), _op(L.H, int(b)),
+                  _op(L.X, n - 1 - int(rng.integers(0, 3))), _op(L.Y, n - 1 - int(rng.integers(0, 3))),
+                  _op(L.CNOT, n - 1, int(c))]
     return np.concatenate([np.asarray(ops, dtype=L.OP_DTYPE), to_array(extra)])
 
 
@@ -76,6 +79,20 @@ def test_sharded_qft_and_parameters():
     params = np.array([0.3, -1.1, 2.4])
     got, _ = _run_local(n, g, pops, params)
     assert np.max(np.abs(got - O.run(n, pops, params))) <= TOL
+
+
+def test_x_and_y_on_global_qubits_move_no_data():
+    # qubits 6 and 7 stay global: X and Y on them, a CNOT and a phase controlled
+    # by them, all without moving data until the relabelling left on qubit 7 is
+    # resolved by the one exchange at the end
+    n, g = 8, 2
+    ops = to_array([_op(L.H, 0), _op(L.H, 1), _op(L.X, 7), _op(L.Y, 6), _op(L.CNOT, 2, 7),
+                    _op(L.CPHASE, 0, 7, 0.4), _op(L.MCPHASE, 1, 0, 0.7, (1 << 6) | (1 << 7)),
+                    _op(L.X, 6), _op(L.RZ, 6, theta=0.9), _op(L.Y, 7), _op(L.X, 7)])
+    got, progs = _run_local(n, g, ops)
+    assert np.max(np.abs(got - O.run(n, ops))) <= TOL
+    assert sum(st[0] == "exchange" for st in progs[0]) == 1
+    assert progs[0][-2][0] == "exchange"
 
 
 def test_local_only_circuits_exchange_nothing():
