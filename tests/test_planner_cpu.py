@@ -11,6 +11,7 @@ import pytest
 
 import oracle_ffi as O
 from quantumsimevo_b200 import _lib as L
+from quantumsimevo_b200 import playground as P
 from quantumsimevo_b200 import workloads as W
 
 NONDIAG = {L.H, L.X, L.Y, L.RX, L.RY, L.GATE2X2, L.CNOT}
@@ -103,6 +104,14 @@ def test_qft_plan_is_few_passes_and_layouts():
     check_plan(14, W.hrz_qft(14, seed=2), 6)
 
 
+def test_playground_circuits_reorder_safely():
+    # Grover's multi-controlled phases and X layers, the TSP XY mixer's H/RX-conjugated ZZ
+    check_plan(10, P.grover(600, iterations=6), 8)
+    dist = [[0, 2, 5], [2, 0, 3], [5, 3, 0]]
+    penalty, gammas, betas = P.tsp_schedule(-1.0, 1.0, 0.8, 0.4, 2, dist)
+    check_plan(9, P.tsp_xy_qaoa(dist, penalty, 1.0, gammas, betas), 6)
+
+
 def test_swaps_are_relabels():
     n = 10
     ops = W.to_array([(L.SWAP, i, n - 1 - i, -1, 0, 0.0, 1.0, (0.0,) * 8) for i in range(n // 2)])
@@ -112,12 +121,20 @@ def test_swaps_are_relabels():
     assert sum(p["nondiag"] for p in plan["passes"]) == 0
 
 
-@pytest.mark.parametrize("name", ["qft16", "random12", "qaoa12_adjoint"])
+@pytest.mark.parametrize("name", ["qft16", "random12", "grover13", "tsp9", "qaoa12_adjoint"])
 def test_generated_pass_kernels_compile(name):
     if name == "qft16":
         n, ops, params, ns = 16, W.hrz_qft(16, seed=2), None, 1
     elif name == "random12":
         n, ops, params, ns = 12, W.random_circuit(12, 200, 5), None, 1
+    elif name == "grover13":
+        # 71 iterations: many passes at the 256-gate cap, few distinct kernels
+        n, ops, params, ns = 13, P.grover(5000), None, 1
+    elif name == "tsp9":
+        n, params, ns = 9, None, 1
+        dist = [[0, 2, 5], [2, 0, 3], [5, 3, 0]]
+        penalty, gammas, betas = P.tsp_schedule(-1.0, 1.0, 0.8, 0.4, 2, dist)
+        ops = P.tsp_xy_qaoa(dist, penalty, 1.0, gammas, betas)
     else:
         ops, params, _, _ = W.qaoa_maxcut(12, 2, seed=3)
         n, ns = 12, 2
