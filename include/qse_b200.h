@@ -218,10 +218,13 @@ QSE_API int qse_execute_mid(qse_state* st, const qse_op* ops, size_t nops, const
                             const double* uniforms, size_t n_uniforms, int32_t* results, size_t n_results);
 
 /* Planner introspection (no device work, no GPU needed): JSON description of
- * the passes Circuit::execute would launch for ops on an n-qubit state with
- * tile_qubits (0 = context default 12) -- per pass the tile qubits and the
- * source-gate order.  Writes at most buflen bytes (NUL-terminated); *needed
- * receives the full length + 1. */
+ * the passes the fusion planner forms for ops on an n-qubit state with
+ * tile_qubits (0 = default 12) and max_gates_per_pass (0 = none) -- per pass
+ * the tile qubits and the source-gate order, each gate as given.  qse_execute
+ * plans the same way, and in addition caps specialised passes at 256
+ * non-diagonal gates and plans each CNOT(c,t) RZ(t) CNOT(c,t) as one diagonal
+ * phase, so its pass count can differ.  Writes at most buflen bytes
+ * (NUL-terminated); *needed receives the full length + 1. */
 QSE_API int qse_plan_describe(uint32_t nqubits, const qse_op* ops, size_t nops, const double* params,
                               size_t nparams, uint32_t tile_qubits, uint32_t max_gates_per_pass,
                               char* buf, size_t buflen, size_t* needed);
