@@ -1,8 +1,8 @@
 """One state sharded over ranks (quantumsimevo_b200/sharded.py) on CPU: the
 lowering (including X and Y on global qubits as relabellings), the half-shard
 exchanges and the final qubit map, with the FP64 oracle as every shard's local
-executor.  All shards in one process (LocalTransport) for
-2, 4 and 8 ranks, and two gloo ranks in two processes (TorchDistTransport)."""
+executor.  All shards in one process (LocalTransport) for 2 to 32 shards, and 2
+and 4 gloo ranks in as many processes (TorchDistTransport)."""
 import math
 import os
 import socket
@@ -68,6 +68,17 @@ def test_sharded_random_circuits_match_oracle(g, seed):
     assert any(st[0] == "exchange" for st in progs[0])
 
 
+@pytest.mark.parametrize("seed", range(12))
+def test_sharded_sweep_small_states(seed):
+    # many small random circuits over 2 to 32 shards (down to two local qubits each)
+    n = 7
+    ops = _mixed(n, 900 + seed)
+    want = O.run(n, ops)
+    for g in (1, 2, 3, 5):
+        got, _ = _run_local(n, g, ops)
+        assert np.max(np.abs(got - want)) <= TOL
+
+
 def test_sharded_qft_and_parameters():
     n, g = 11, 2
     ops = to_array(W.qft_ops(n))
@@ -121,7 +132,7 @@ def _worker(rank, world, port, outdir):
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
-        n, g = 10, 1
+        n, g = 10, world.bit_length() - 1
         nl = n - g
         ops = _mixed(n, 705)
         steps, pos = S.lower(ops, n, g, rank)
@@ -139,8 +150,8 @@ def _worker(rank, world, port, outdir):
         dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_exchange_halves(tmp_path):
-    world = 2
+@pytest.mark.parametrize("world", [2, 4])
+def test_gloo_ranks_exchange_halves(tmp_path, world):
     ctx = mp.get_context("spawn")
     port = _free_port()
     procs = [ctx.Process(target=_worker, args=(r, world, port, str(tmp_path))) for r in range(world)]
@@ -153,7 +164,7 @@ def test_two_gloo_ranks_exchange_halves(tmp_path):
             pytest.fail("rank did not finish")
         assert p.exitcode == 0
     d = [np.load(tmp_path / f"r{r}.npz") for r in range(world)]
-    assert np.array_equal(d[0]["pos"], d[1]["pos"])
+    assert all(np.array_equal(d[0]["pos"], x["pos"]) for x in d)
     n = 10
-    got = S.logical_order([d[0]["shard"], d[1]["shard"]], n, 1, list(d[0]["pos"]))
+    got = S.logical_order([x["shard"] for x in d], n, world.bit_length() - 1, list(d[0]["pos"]))
     assert np.max(np.abs(got - O.run(n, _mixed(n, 705)))) <= TOL
