@@ -8,7 +8,6 @@ import numpy as np
 import pytest
 
 import oracle_ffi as O
-from quantumsimevo_b200 import _lib as L
 from quantumsimevo_b200 import sharded as S
 from quantumsimevo_b200 import workloads as W
 from quantumsimevo_b200.circuit import Circuit, Device
