@@ -15,8 +15,11 @@
 //     sums fit, larger observables are rejected with QSE_ERR_SIZE;
 //   - every call on a device shares the array: a call writes all the partial
 //     sums it reads and the term table it uses, so nothing has to start at
-//     zero, but two calls whose work overlaps on the GPU (other streams,
-//     other contexts of the same device) race on it;
+//     zero, but any two calls on one device that run at the same time race on
+//     it: calls from several host threads (on one context or several), and
+//     calls whose GPU work overlaps (other streams, other contexts);
+//   - the call is synchronous: it returns after its result has reached the
+//     host (it waits on the context's stream);
 //   - the first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (the host-side name of a __device__ array is not a
 //     device address); make that first call before any stream capture.
@@ -52,18 +55,25 @@ char* scratch_address(int device)
     return static_cast<char*>(g_scratch_dev[device]);
 }
 
-// partial[b] = sum over the block's amplitudes of O(x)|psi_x|^2
+// partial[b] = sum over the block's amplitudes of O(x)|psi_x|^2; the term
+// table (at most kMaxTerms entries, 32 KiB) is staged in static shared memory
+// once per block, as qse_expectation's kernel does, so the inner loop over
+// the terms reads shared memory instead of global memory
 __global__ void __launch_bounds__(kThreads) k_expect_noalloc(const double2* __restrict__ psi, uint64_t size,
                                                              const uint64_t* __restrict__ z,
                                                              const double* __restrict__ w, uint32_t nt, double c,
                                                              double* __restrict__ partial)
 {
     __shared__ double sh[kThreads / 32];
+    __shared__ uint64_t sz[kMaxTerms];
+    __shared__ double sw[kMaxTerms];
+    for (uint32_t t = threadIdx.x; t < nt; t += blockDim.x) { sz[t] = z[t]; sw[t] = w[t]; }
+    __syncthreads();
     double acc = 0.0;
     for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < size; i += uint64_t(gridDim.x) * blockDim.x) {
         const double2 v = psi[i];
         double o = c;
-        for (uint32_t t = 0; t < nt; ++t) o += (__popcll(i & z[t]) & 1) ? -w[t] : w[t];
+        for (uint32_t t = 0; t < nt; ++t) o += (__popcll(i & sz[t]) & 1) ? -sw[t] : sw[t];
         acc += o * (v.x * v.x + v.y * v.y);
     }
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);

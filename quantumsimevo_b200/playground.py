@@ -13,7 +13,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import CNOT, CPHASE, H, MCPHASE, RX, RZ, SWAP, X
+from .abi import CNOT, CPHASE, H, MCPHASE, RX, RZ, SWAP, X
 from .workloads import _op, to_array
 
 PI = 3.14159265358979323846   # Grover.cpp:10, QFT.cpp:6

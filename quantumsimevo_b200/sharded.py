@@ -235,8 +235,12 @@ class TorchDistTransport:
         x = self.t.view(1 << (nl - l - 1), 2, 1 << l)
         send = torch.view_as_real(x[:, 1 - b, :].contiguous())
         recv = torch.empty_like(send)
-        reqs = [self.dist.isend(send, partner, group=self.group), self.dist.irecv(recv, partner, group=self.group)]
-        for rq in reqs:
+        # one grouped send+receive: under NCCL both partners' sends and receives
+        # are posted together (a send issued alone would wait for a receive that
+        # sits queued behind the partner's own send on the same stream)
+        ops = [self.dist.P2POp(self.dist.isend, send, partner, group=self.group),
+               self.dist.P2POp(self.dist.irecv, recv, partner, group=self.group)]
+        for rq in self.dist.batch_isend_irecv(ops):
             rq.wait()
         x[:, 1 - b, :] = torch.view_as_complex(recv)
 

@@ -17,7 +17,7 @@ import math
 
 import numpy as np
 
-from ._lib import (CNOT, CPHASE, GATE2X2, H, MCPHASE, OP_DTYPE, PHASE, RX, RY, RZ, SWAP, X, Y, Z)
+from .abi import (CNOT, CPHASE, GATE2X2, H, MCPHASE, OP_DTYPE, PHASE, RX, RY, RZ, SWAP, X, Y, Z)
 
 MASK64 = (1 << 64) - 1
 TWO_PI = 2.0 * math.pi

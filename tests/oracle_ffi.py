@@ -7,7 +7,7 @@ import os
 
 import numpy as np
 
-from quantumsimevo_b200._lib import OP_DTYPE, QseNoiseConfig, QseObservable
+from quantumsimevo_b200.abi import OP_DTYPE, QseNoiseConfig, QseObservable
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_PATH = os.path.join(ROOT, "oracle", "libqse_oracle.so")
