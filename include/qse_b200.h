@@ -330,6 +330,13 @@ typedef struct qse_batch_config {
                                per SM); 0: 128 registers (two CTAs of 256 per SM)         */
 } qse_batch_config;
 QSE_API int qse_batch_set_config(qse_batch* b, const qse_batch_config* cfg);
+/* Bound of the persistent kernel's dependency waits: a work item polls the
+ * completion counter of the pass it depends on at most `polls` times (with
+ * back-off) before it gives up; then every CTA stops claiming work and the run
+ * returns QSE_ERR_TIMEOUT (results invalid, the batch stays usable).
+ * 0 restores the default (2^21 polls, about a second).  No reference
+ * counterpart (failure detection of the batched kernel). */
+QSE_API int qse_batch_set_wait_limit(qse_batch* b, uint32_t polls);
 QSE_API int qse_batch_get_config(const qse_batch* b, qse_batch_config* cfg);
 
 typedef struct qse_batch_stats {

@@ -9,6 +9,13 @@
  * scales both parts), and this file is compiled with -ffp-contract=off, so the
  * gate results match the reference scalar backend bit for bit.
  *
+ * Element-wise gate loops run under OpenMP (every iteration writes its own
+ * amplitudes, so the results do not depend on the thread count); the
+ * expectation and gradient sums use a fixed chunked order (the same bits for
+ * any thread count); reductions that the reference performs in index order
+ * (cumulative sums, measure's running sum, measureQubit's probability) stay
+ * sequential.
+ *
  * Pinning: tests/test_oracle_kat.py checks these functions against the
  * QSETests known answers; tests/test_oracle_vs_reference.py against the
  * reference sources compiled into oracle/_ref.
@@ -33,6 +40,18 @@ static inline double cnorm(cplx a) { return a.re * a.re + a.im * a.im; }
 
 #define AMP(st, i) (((cplx*)(st))[i])
 
+/* Reductions under OpenMP in a fixed order: kChunks contiguous index ranges
+ * summed in parallel, then the chunk sums in chunk order -- the same bits for
+ * every thread count and every run. */
+enum { kChunks = 256 };
+static size_t chunk_len(size_t size) { return (size + kChunks - 1) / kChunks; }
+static double sum_parts(const double* part)
+{
+    double acc = 0.0;
+    for (int c = 0; c < kChunks; ++c) acc += part[c];
+    return acc;
+}
+
 void orc_init(double* st, unsigned n)
 {
     /* StateVector.cpp:14-27: zero fill, amplitude 0 = 1 */
@@ -45,6 +64,7 @@ void orc_init(double* st, unsigned n)
 static void g_2x2(double* st, unsigned n, const cplx g[4], unsigned q)
 {
     size_t size = (size_t)1 << n, sec = (size_t)1 << q;
+    #pragma omp parallel for schedule(static)
     for (size_t i = 0; i < (size >> 1); ++i) {
         size_t i0 = ((i >> q) << (q + 1)) | (i & (sec - 1));
         size_t i1 = i0 | sec;
@@ -58,6 +78,7 @@ static void g_2x2(double* st, unsigned n, const cplx g[4], unsigned q)
 static void g_cnot(double* st, unsigned n, unsigned c, unsigned t)
 {
     size_t size = (size_t)1 << n, cm = (size_t)1 << c, tm = (size_t)1 << t;
+    #pragma omp parallel for schedule(static)
     for (size_t i = 0; i < size; ++i)
         if ((i & cm) && (i < (i ^ tm))) {
             cplx tmp = AMP(st, i);
@@ -70,6 +91,7 @@ static void g_cnot(double* st, unsigned n, unsigned c, unsigned t)
 static void g_x(double* st, unsigned n, unsigned q)
 {
     size_t size = (size_t)1 << n, m = (size_t)1 << q;
+    #pragma omp parallel for schedule(static)
     for (size_t i = 0; i < size; ++i)
         if (!(i & m)) {
             cplx tmp = AMP(st, i);
@@ -83,12 +105,15 @@ static void g_h(double* st, unsigned n, unsigned q)
 {
     const double s = 0.7071067811865475244;
     size_t size = (size_t)1 << n, step = (size_t)1 << q;
-    for (size_t i = 0; i < size; i += 2 * step)
-        for (size_t j = i; j < i + step; ++j) {
-            cplx v0 = AMP(st, j), v1 = AMP(st, j + step);
-            AMP(st, j) = cscl(s, cadd(v0, v1));
-            AMP(st, j + step) = cscl(s, csub(v0, v1));
-        }
+    /* the reference's blocked double loop visits each pair (j, j + step) once;
+     * the same pairs as one flat loop over pair indices */
+    #pragma omp parallel for schedule(static)
+    for (size_t k = 0; k < (size >> 1); ++k) {
+        size_t j = ((k >> q) << (q + 1)) | (k & (step - 1));
+        cplx v0 = AMP(st, j), v1 = AMP(st, j + step);
+        AMP(st, j) = cscl(s, cadd(v0, v1));
+        AMP(st, j + step) = cscl(s, csub(v0, v1));
+    }
 }
 
 /* CircuitUnitaryOperation.cpp:112-132 (applyPhase) */
@@ -96,6 +121,7 @@ static void g_phase(double* st, unsigned n, unsigned q, double theta)
 {
     size_t size = (size_t)1 << n, m = (size_t)1 << q;
     cplx ph = cexpi(theta);
+    #pragma omp parallel for schedule(static)
     for (size_t i = 0; i < size; ++i)
         if (i & m) AMP(st, i) = cmul(AMP(st, i), ph);
 }
@@ -105,6 +131,7 @@ static void g_y(double* st, unsigned n, unsigned q)
 {
     size_t size = (size_t)1 << n, m = (size_t)1 << q;
     const cplx I = cmk(0.0, 1.0), mI = cmk(-0.0, -1.0);
+    #pragma omp parallel for schedule(static)
     for (size_t i = 0; i < size; ++i)
         if (!(i & m)) {
             cplx v0 = AMP(st, i), v1 = AMP(st, i | m);
@@ -118,6 +145,7 @@ static void g_y(double* st, unsigned n, unsigned q)
 static void g_z(double* st, unsigned n, unsigned q)
 {
     size_t size = (size_t)1 << n, m = (size_t)1 << q;
+#pragma omp parallel for schedule(static)
     for (size_t i = 0; i < size; ++i)
         if (i & m) AMP(st, i) = cmk(-AMP(st, i).re, -AMP(st, i).im);
 }
@@ -128,6 +156,7 @@ static void g_rx(double* st, unsigned n, unsigned q, double theta)
     size_t size = (size_t)1 << n, m = (size_t)1 << q;
     double c = cos(theta / 2.0), s = sin(theta / 2.0);
     cplx miS = cmk(0.0, -s);
+    #pragma omp parallel for schedule(static)
     for (size_t i = 0; i < size; ++i)
         if (!(i & m)) {
             cplx v0 = AMP(st, i), v1 = AMP(st, i | m);
@@ -141,6 +170,7 @@ static void g_ry(double* st, unsigned n, unsigned q, double theta)
 {
     size_t size = (size_t)1 << n, m = (size_t)1 << q;
     double c = cos(theta / 2.0), s = sin(theta / 2.0);
+    #pragma omp parallel for schedule(static)
     for (size_t i = 0; i < size; ++i)
         if (!(i & m)) {
             cplx v0 = AMP(st, i), v1 = AMP(st, i | m);
@@ -154,6 +184,7 @@ static void g_rz(double* st, unsigned n, unsigned q, double theta)
 {
     size_t size = (size_t)1 << n, m = (size_t)1 << q;
     cplx p0 = cexpi(-theta / 2.0), p1 = cexpi(theta / 2.0);
+    #pragma omp parallel for schedule(static)
     for (size_t i = 0; i < size; ++i)
         AMP(st, i) = cmul(AMP(st, i), (i & m) ? p1 : p0);
 }
@@ -164,6 +195,7 @@ static void g_swap(double* st, unsigned n, unsigned q0, unsigned q1)
     size_t size = (size_t)1 << n, m0 = (size_t)1 << q0, m1 = (size_t)1 << q1;
     unsigned lo = q0 < q1 ? q0 : q1, hi = q0 < q1 ? q1 : q0;
     size_t low_mask = ((size_t)1 << lo) - 1;
+    #pragma omp parallel for schedule(static)
     for (size_t k = 0; k < size / 4; ++k) {
         size_t i = ((k >> lo) << (lo + 1)) | (k & low_mask);
         size_t idx = ((i >> hi) << (hi + 1)) | (i & (((size_t)1 << hi) - 1));
@@ -178,6 +210,7 @@ static void g_mcphase(double* st, unsigned n, uint64_t all_mask, double theta)
 {
     size_t size = (size_t)1 << n;
     cplx ph = cexpi(theta);
+    #pragma omp parallel for schedule(static)
     for (size_t i = 0; i < size; ++i)
         if (((uint64_t)i & all_mask) == all_mask) AMP(st, i) = cmul(AMP(st, i), ph);
 }
@@ -187,6 +220,7 @@ static void g_cphase(double* st, unsigned n, unsigned c, unsigned t, double thet
 {
     size_t size = (size_t)1 << n, cm = (size_t)1 << c, tm = (size_t)1 << t;
     double co = cos(theta), si = sin(theta);
+    #pragma omp parallel for schedule(static)
     for (size_t i = 0; i < size; ++i)
         if ((i & cm) && (i & tm)) {
             double re = AMP(st, i).re, im = AMP(st, i).im;
@@ -282,6 +316,31 @@ void orc_sample(const double* st, unsigned n, const double* u, size_t nshots, ui
         out[s] = orc_lower_bound(cum, size, target);
     }
     free(cum);
+}
+
+/* orc_sample, and in the same cumulative array (one build: at 30 qubits it
+ * is 8 GiB) the number of draws whose target lies within `ulps` units in the
+ * last place of the cumulative value at or just below the chosen index --
+ * the draws where a differently rounded prefix sum could pick a neighbour. */
+size_t orc_sample_margin(const double* st, unsigned n, const double* u, size_t nshots, uint64_t* out, double ulps)
+{
+    size_t size = (size_t)1 << n;
+    double* cum = (double*)malloc(size * sizeof(double));
+    if (!cum) return (size_t)-1;
+    orc_cdf(st, n, cum);
+    double total = cum[size - 1];
+    size_t near = 0;
+    for (size_t s = 0; s < nshots; ++s) {
+        double target = u[s] * (total - 0.0) + 0.0;
+        size_t i = orc_lower_bound(cum, size, target);
+        out[s] = i;
+        double c_hi = i < size ? cum[i] : total;
+        double c_lo = i > 0 ? cum[i - 1] : 0.0;
+        double tol = ulps * (nextafter(target, INFINITY) - target);
+        if (fabs(c_hi - target) <= tol || fabs(target - c_lo) <= tol) ++near;
+    }
+    free(cum);
+    return near;
 }
 
 /* StateVector.cpp:118-156 with the draw injected.  The total is the
@@ -500,9 +559,16 @@ double orc_obs_value(uint64_t x, const qse_observable* obs)
 double orc_expectation(const double* st, unsigned n, const qse_observable* obs)
 {
     size_t size = (size_t)1 << n;
-    double acc = 0.0;
-    for (size_t i = 0; i < size; ++i) acc += cnorm(AMP(st, i)) * orc_obs_value(i, obs);
-    return acc;
+    double part[kChunks];
+    const size_t len = chunk_len(size);
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < kChunks; ++c) {
+        double acc = 0.0;
+        for (size_t i = (size_t)c * len; i < size && i < (size_t)(c + 1) * len; ++i)
+            acc += cnorm(AMP(st, i)) * orc_obs_value(i, obs);
+        part[c] = acc;
+    }
+    return sum_parts(part);
 }
 
 /* inverse of one gate (all gate types of the reference are unitary) */
@@ -540,6 +606,7 @@ static int apply_derivative(double* mu, const double* psi, unsigned n, const qse
         cplx d[4];
         if (op->type == QSE_GATE_RX) { d[0] = cmk(-s / 2, 0); d[1] = cmk(0, -c / 2); d[2] = cmk(0, -c / 2); d[3] = cmk(-s / 2, 0); }
         else { d[0] = cmk(-s / 2, 0); d[1] = cmk(-c / 2, 0); d[2] = cmk(c / 2, 0); d[3] = cmk(-s / 2, 0); }
+#pragma omp parallel for schedule(static)
         for (size_t i = 0; i < size; ++i)
             if (!(i & m)) {
                 cplx v0 = AMP(psi, i), v1 = AMP(psi, i | m);
@@ -550,6 +617,7 @@ static int apply_derivative(double* mu, const double* psi, unsigned n, const qse
     }
     case QSE_GATE_RZ: {
         cplx d0 = cmul(cmk(0, -0.5), cexpi(-theta / 2)), d1 = cmul(cmk(0, 0.5), cexpi(theta / 2));
+#pragma omp parallel for schedule(static)
         for (size_t i = 0; i < size; ++i) AMP(mu, i) = cmul(AMP(psi, i), (i & m) ? d1 : d0);
         return 0;
     }
@@ -558,6 +626,7 @@ static int apply_derivative(double* mu, const double* psi, unsigned n, const qse
         if (op->type == QSE_GATE_CPHASE) all |= (uint64_t)1 << op->control;
         if (op->type == QSE_GATE_MCPHASE) all |= op->controls;
         cplx d = cmul(cmk(0, 1), cexpi(theta));
+#pragma omp parallel for schedule(static)
         for (size_t i = 0; i < size; ++i)
             if (((uint64_t)i & all) == all) AMP(mu, i) = cmul(AMP(psi, i), d);
         return 0;
@@ -578,21 +647,33 @@ double orc_adjoint(unsigned n, const qse_op* ops, size_t nops, const double* par
     for (size_t p = 0; p < nparams; ++p) grad[p] = 0.0;
     orc_init(psi, n);
     orc_run(psi, n, ops, nops, params);
-    double value = 0.0;
-    for (size_t i = 0; i < size; ++i) {
-        double o = orc_obs_value(i, obs);
-        AMP(lam, i) = cscl(o, AMP(psi, i));
-        value += cnorm(AMP(psi, i)) * o;
+    double part[kChunks];
+    const size_t len = chunk_len(size);
+#pragma omp parallel for schedule(static)
+    for (int c = 0; c < kChunks; ++c) {
+        double acc = 0.0;
+        for (size_t i = (size_t)c * len; i < size && i < (size_t)(c + 1) * len; ++i) {
+            double o = orc_obs_value(i, obs);
+            AMP(lam, i) = cscl(o, AMP(psi, i));
+            acc += cnorm(AMP(psi, i)) * o;
+        }
+        part[c] = acc;
     }
+    double value = sum_parts(part);
     for (size_t k = nops; k-- > 0;) {
         const qse_op* op = &ops[k];
         double th = bound_angle(op, params);
         apply_inverse(psi, n, op, th);
         if (op->param >= 0 && (size_t)op->param < nparams) {
             apply_derivative(mu, psi, n, op, th);
-            double acc = 0.0;
-            for (size_t i = 0; i < size; ++i) acc += AMP(lam, i).re * AMP(mu, i).re + AMP(lam, i).im * AMP(mu, i).im;
-            grad[op->param] += op->coeff * 2.0 * acc;
+#pragma omp parallel for schedule(static)
+            for (int c = 0; c < kChunks; ++c) {
+                double acc = 0.0;
+                for (size_t i = (size_t)c * len; i < size && i < (size_t)(c + 1) * len; ++i)
+                    acc += AMP(lam, i).re * AMP(mu, i).re + AMP(lam, i).im * AMP(mu, i).im;
+                part[c] = acc;
+            }
+            grad[op->param] += op->coeff * 2.0 * sum_parts(part);
         }
         apply_inverse(lam, n, op, th);
     }

@@ -29,6 +29,9 @@ int  orc_run(double* st, unsigned n, const qse_op* ops, size_t nops, const doubl
 void   orc_cdf(const double* st, unsigned n, double* cum);
 size_t orc_lower_bound(const double* cum, size_t size, double target);
 void   orc_sample(const double* st, unsigned n, const double* u, size_t nshots, uint64_t* out);
+/* orc_sample plus the count of draws within `ulps` ulps of a cumulative boundary;
+ * (size_t)-1 if the cumulative array cannot be allocated */
+size_t orc_sample_margin(const double* st, unsigned n, const double* u, size_t nshots, uint64_t* out, double ulps);
 uint64_t orc_measure(double* st, unsigned n, double u);
 /* StateVector::measureQubit / resetQubit (StateVector.cpp:158-221), draw injected;
  * return the outcome, *prob1 = the probability of the qubit being 1 */

@@ -371,6 +371,25 @@ void ref_statevector_reset_qubit(void* svp, unsigned qubit)
     static_cast<StateVector*>(svp)->resetQubit(qubit);
 }
 
+// StateVector::reset (StateVector.cpp:34-46): |0..0> on the host copy.
+void ref_statevector_reset(void* svp)
+{
+    Quiet q(true);
+    static_cast<StateVector*>(svp)->reset();
+}
+
+// Waits for every kernel the reference CUDA backend has queued (it launches
+// on a private stream and synchronises only in flush or print_steps timing);
+// lets the bench time its kernels without a state copy.  0 on success.
+int ref_device_synchronize(void)
+{
+#ifdef QSE_REF_WITH_GPU
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1;
+#else
+    return -1;
+#endif
+}
+
 void ref_statevector_sample(void* svp, int shots, uint64_t* out)
 {
     Quiet q(g_quiet);

@@ -89,6 +89,7 @@ _SIGS = {
     "qse_batch_autotune": ([_vp, C.c_char_p], C.c_int),
     "qse_batch_use_graph": ([_vp, C.c_int], C.c_int),
     "qse_batch_set_config": ([_vp, C.POINTER(QseBatchConfig)], C.c_int),
+    "qse_batch_set_wait_limit": ([_vp, _u32], C.c_int),
     "qse_batch_get_config": ([_vp, C.POINTER(QseBatchConfig)], C.c_int),
     "qse_batch_get_stats": ([_vp, C.POINTER(QseBatchStats)], C.c_int),
 }

@@ -85,6 +85,11 @@ class Batch:
         check(lib.qse_batch_autotune(self.handle, cache_path.encode() if cache_path else None))
         return self.config
 
+    def set_wait_limit(self, polls: int = 0) -> None:
+        """Polls before a dependency wait of the persistent kernel gives up
+        (the run then raises QseError with status TIMEOUT); 0 = the default."""
+        check(lib.qse_batch_set_wait_limit(self.handle, int(polls)))
+
     def use_graph(self, enabled: bool = True) -> None:
         check(lib.qse_batch_use_graph(self.handle, 1 if enabled else 0))
 

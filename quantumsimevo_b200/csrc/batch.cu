@@ -119,6 +119,9 @@ struct BatchArgs {
 };
 
 constexpr uint32_t kMaxThreads = 512;
+// polls (with back-off up to 2 us each) before a work item's dependency wait
+// gives up: about a second, far beyond any pass of a circuit that fits
+constexpr uint32_t kDefaultWaitPolls = 1u << 21;
 
 // exchange buffer | group values | per-warp gradient partials | warp sums
 size_t smem_bytes(uint32_t kmax, uint32_t max_groups, uint32_t max_slots, uint32_t threads)
@@ -432,6 +435,7 @@ struct qse_batch {
     Config cfg;
     bool use_graph = true;
     bool built = false;
+    uint32_t wait_limit = 0;      // polls before a dependency wait gives up, 0 = kDefaultWaitPolls
     std::vector<double> last_params;
 
     qse::DevBuf prog, work, pool;
@@ -759,7 +763,7 @@ void build(qse_batch* b)
     A.kmax = kmax;
     A.max_groups = max_groups;
     A.max_slots = max_slots;
-    A.spin_limit = 1u << 21;
+    A.spin_limit = b->wait_limit ? b->wait_limit : kDefaultWaitPolls;
     b->d_ops = reinterpret_cast<plan::KOp*>(pd + o_ops);
     b->d_terms = reinterpret_cast<plan::TermRec*>(pd + o_terms);
     b->patches = reinterpret_cast<const BPatch*>(pd + o_pt);
@@ -1121,6 +1125,18 @@ int qse_batch_use_graph(qse_batch* b, int enabled)
     if (!b) qse::fail(QSE_ERR_INVALID, "null batch");
     b->use_graph = enabled != 0;
     drop_graph(b);
+    QSE_BATCH_GUARD_END
+}
+
+int qse_batch_set_wait_limit(qse_batch* b, uint32_t polls)
+{
+    QSE_BATCH_GUARD_BEGIN
+    if (!b) qse::fail(QSE_ERR_INVALID, "null batch");
+    QSE_CUDA(cudaSetDevice(b->ctx->device));
+    QSE_CUDA(cudaStreamSynchronize(b->ctx->stream));
+    b->wait_limit = polls;
+    b->args.spin_limit = polls ? polls : kDefaultWaitPolls;
+    drop_graph(b);   // the graph holds the kernel's arguments by value
     QSE_BATCH_GUARD_END
 }
 

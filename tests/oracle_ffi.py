@@ -31,6 +31,7 @@ def _load_oracle():
         "orc_run": ([_vp, C.c_uint, _vp, _sz, _pd], C.c_int),
         "orc_cdf": ([_vp, C.c_uint, _pd], None),
         "orc_sample": ([_vp, C.c_uint, _pd, _sz, _pu64], None),
+        "orc_sample_margin": ([_vp, C.c_uint, _pd, _sz, _pu64, _d], _sz),
         "orc_measure": ([_vp, C.c_uint, _d], _u64),
         "orc_mt_seed": ([_vp, _u32], None),
         "orc_mt_next": ([_vp], _u32),
@@ -109,6 +110,24 @@ def sample(st, n, u):
     return out
 
 
+def sample_margin(st, n, u, ulps=4.0):
+    """(outcomes, number of draws within `ulps` ulps of a cumulative boundary),
+    one cumulative array (no copy of the state)."""
+    st = np.ascontiguousarray(st, dtype=np.complex128)
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    out = np.empty(u.size, dtype=np.uint64)
+    near = oracle.orc_sample_margin(st.ctypes.data_as(_vp), n, u.ctypes.data_as(_pd), u.size,
+                                    out.ctypes.data_as(_pu64), float(ulps))
+    assert near != C.c_size_t(-1).value, "oracle could not allocate the cumulative array"
+    return out, int(near)
+
+
+def measure_in_place(st, n, u):
+    """orc_measure on st itself (collapsed in place; no copy of a large state)."""
+    assert st.flags["C_CONTIGUOUS"] and st.dtype == np.complex128
+    return int(oracle.orc_measure(st.ctypes.data_as(_vp), n, float(u)))
+
+
 def cdf(st, n):
     st = np.ascontiguousarray(st, dtype=np.complex128)
     out = np.empty(1 << n, dtype=np.float64)
@@ -134,6 +153,15 @@ def adjoint(n, ops, params, obs):
     v = oracle.orc_adjoint(n, a.ctypes.data_as(_vp), len(a), p.ctypes.data_as(_pd), p.size, C.byref(obs),
                            g.ctypes.data_as(_pd))
     return v, g
+
+
+def adjoint_job(args):
+    """adjoint() on (n, ops, params, (zmasks, weights, constant)): picklable, for worker processes."""
+    n, ops, params, (zm, w, c) = args
+    z = np.ascontiguousarray(np.asarray(zm, dtype=np.uint64))
+    wt = np.ascontiguousarray(np.asarray(w, dtype=np.float64))
+    obs = QseObservable(len(z), z.ctypes.data_as(_pu64), wt.ctypes.data_as(_pd), float(c))
+    return adjoint(n, ops, params, obs)
 
 
 def param_shift(n, ops, params, obs):

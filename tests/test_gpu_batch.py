@@ -226,3 +226,27 @@ def test_hea_512_finite_differences(dev):
         vw, gw = O.adjoint(circs[i][0], circs[i][1], params[off[i]:off[i + 1]], obs)
         assert abs(v[i] - vw) <= TOL
         assert np.max(np.abs(g[off[i]:off[i + 1]] - gw)) <= TOL
+
+
+def test_bounded_wait_gives_up_and_batch_recovers(dev):
+    """The persistent kernel's dependency waits are bounded.  With a limit of one
+    poll, a dependent work item of a multi-tile queue finds its pass unfinished
+    and gives up: it sets the error word, every CTA stops claiming work and
+    leaves, and the run returns QSE_ERR_TIMEOUT -- no kernel keeps waiting and
+    nothing faults.  The next run with the default limit matches the oracle."""
+    circs, params = hea(4, 18, 18, 3, 3, seed=77)   # 18 qubits: 128 tiles per pass at the default tile
+    b = Batch(circs, dev)
+    b.set_wait_limit(1)
+    gave_up = 0
+    for _ in range(3):
+        try:
+            b.run(params)
+        except L.QseError as e:
+            assert e.status == 7, e   # QSE_ERR_TIMEOUT
+            gave_up += 1
+    assert gave_up >= 1
+    b.set_wait_limit(0)
+    v, g = b.run(params)
+    vw, gw = oracle_all(circs, params)
+    assert np.max(np.abs(v - vw)) <= TOL
+    assert np.max(np.abs(g - gw)) <= TOL
