@@ -7,6 +7,12 @@
 // an explicit choice, and exposes the reference Circuit through extern "C"
 // so Python tests and bench.py's reference arm can drive it.
 //
+// Built three ways: libqse_ref_cpu.so (CPU backends), libqse_ref_gpu.so (+ the
+// reference CUDA backend and the B200 adapter), libqse_ref_patched.so (the GPU
+// build over a copy of the reference tree whose interface and Circuit carry the
+// optional executeProgram / sample / measure hooks, oracle/patch_reference.py;
+// QSE_REF_PATCHED).
+//
 // Backends: 0 = scalar CircuitUnitaryOperation (the FP64 oracle of record),
 //           1 = CircuitUnitaryOperationAVX (the timed CPU baseline),
 //           2 = CircuitUnitaryOperationGPU rebuilt for sm_100a (only in libqse_ref_gpu.so),
@@ -282,7 +288,8 @@ int ref_b200_sample(void* be, void* svp, const double* u, size_t shots, uint64_t
 #ifdef QSE_REF_WITH_GPU
     auto* b = dynamic_cast<CircuitUnitaryOperationB200*>(static_cast<ICircuitUnitaryOperation*>(be));
     if (!b) return -1;
-    std::vector<size_t> r = b->sample(*static_cast<StateVector*>(svp), u, shots);
+    std::vector<size_t> r;
+    b->sample(*static_cast<StateVector*>(svp), u, shots, r);
     for (size_t i = 0; i < r.size(); ++i) out[i] = r[i];
     return 0;
 #else
@@ -296,7 +303,9 @@ int ref_b200_measure(void* be, void* svp, double u, uint64_t* out)
 #ifdef QSE_REF_WITH_GPU
     auto* b = dynamic_cast<CircuitUnitaryOperationB200*>(static_cast<ICircuitUnitaryOperation*>(be));
     if (!b) return -1;
-    *out = b->measure(*static_cast<StateVector*>(svp), u);
+    size_t r = 0;
+    b->measure(*static_cast<StateVector*>(svp), u, r);
+    *out = r;
     return 0;
 #else
     (void)be; (void)svp; (void)u; (void)out;
@@ -370,6 +379,29 @@ void ref_statevector_reset_qubit(void* svp, unsigned qubit)
     Quiet q(true);
     static_cast<StateVector*>(svp)->resetQubit(qubit);
 }
+
+#ifdef QSE_REF_PATCHED
+// Draw source of the patched Circuit::sample / Circuit::measure
+// (oracle/patch_reference.py): injected uniforms first, then a generator seeded
+// from std::random_device like the reference's own draws.
+namespace {
+std::vector<double> g_injected;
+size_t g_injected_next = 0;
+}  // namespace
+}  // extern "C"
+double qse_patch_next_uniform()
+{
+    if (g_injected_next < g_injected.size()) return g_injected[g_injected_next++];
+    static std::mt19937 gen{std::random_device{}()};
+    return std::uniform_real_distribution<double>(0.0, 1.0)(gen);
+}
+extern "C" {
+void ref_inject_uniforms(const double* u, size_t n)
+{
+    g_injected.assign(u, u + n);
+    g_injected_next = 0;
+}
+#endif
 
 // StateVector::reset (StateVector.cpp:34-46): |0..0> on the host copy.
 void ref_statevector_reset(void* svp)

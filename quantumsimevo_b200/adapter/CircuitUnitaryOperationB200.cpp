@@ -149,7 +149,7 @@ void CircuitUnitaryOperationB200::applySwap(StateVector& sv, size_t q0, size_t q
     QSE_TIMED("Swap", qse_apply_swap(state_, uint32_t(q0), uint32_t(q1)));
 }
 
-void CircuitUnitaryOperationB200::executeProgram(StateVector& sv, const std::vector<GateCommand>& commands)
+bool CircuitUnitaryOperationB200::executeProgram(StateVector& sv, const std::vector<GateCommand>& commands)
 {
     ensureOnDevice(sv);
     std::vector<qse_op> ops;
@@ -166,20 +166,24 @@ void CircuitUnitaryOperationB200::executeProgram(StateVector& sv, const std::vec
     }
     qse_exec_stats stats{};
     QSE_TIMED("Program", qse_execute(state_, ops.data(), ops.size(), nullptr, 0, nullptr, nullptr, 0, &stats));
+    return true;
 }
 
-std::vector<size_t> CircuitUnitaryOperationB200::sample(StateVector& sv, const double* uniforms, size_t shots)
+bool CircuitUnitaryOperationB200::sample(StateVector& sv, const double* uniforms, size_t shots,
+                                         std::vector<size_t>& out)
 {
     ensureOnDevice(sv);
-    std::vector<uint64_t> out(shots);
-    if (shots) check(qse_sample(state_, uniforms, shots, 0, out.data()), "qse_sample");
-    return std::vector<size_t>(out.begin(), out.end());
+    std::vector<uint64_t> idx(shots);
+    if (shots) check(qse_sample(state_, uniforms, shots, 0, idx.data()), "qse_sample");
+    out.assign(idx.begin(), idx.end());
+    return true;
 }
 
-size_t CircuitUnitaryOperationB200::measure(StateVector& sv, double u)
+bool CircuitUnitaryOperationB200::measure(StateVector& sv, double u, size_t& out)
 {
     ensureOnDevice(sv);
     uint64_t idx = 0;
     check(qse_measure(state_, u, &idx), "qse_measure");
-    return static_cast<size_t>(idx);
+    out = static_cast<size_t>(idx);
+    return true;
 }

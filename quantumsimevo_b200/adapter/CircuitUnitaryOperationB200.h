@@ -41,19 +41,25 @@ public:
     void flush() override;
     void markHostDirty() override;
 
-    // Extension used by a Circuit::execute that hands over its whole queue
-    // (the fusion planner path): one call, any number of passes.
-    void executeProgram(StateVector& sv, const std::vector<GateCommand>& commands);
+    // Optional hooks a Circuit can call when the interface declares them as
+    // virtuals with declining defaults (the test build compiles such a patched
+    // ICircuitUnitaryOperation.h and Circuit.cpp, oracle/patch_reference.py).
+    // Against the unpatched interface they are plain members.  Each returns
+    // true: it handled the call.
+    //
+    // executeProgram: Circuit::execute's whole queue (Circuit.cpp:64-120,
+    // noise off) through the fusion planner -- one call, any number of passes.
+    bool executeProgram(StateVector& sv, const std::vector<GateCommand>& commands);
 
-    // Extensions for Circuit::sample / Circuit::measure (StateVector.cpp:77-156)
-    // on the device copy, so neither needs the full-state copy to the host.
-    // Each shot / the measurement takes its uniform draw u in [0, 1) from the
-    // caller (the reference draws from std::random_device); the outcome is the
-    // one StateVector::sample / measure gives for the same draw.  measure()
+    // Circuit::sample / Circuit::measure (StateVector.cpp:77-156) on the device
+    // copy, so neither needs the full-state copy to the host.  Each shot / the
+    // measurement takes its uniform draw u in [0, 1) from the caller (the
+    // reference draws from std::random_device); the outcome is the one
+    // StateVector::sample / measure gives for the same draw.  measure()
     // collapses the device copy, which stays authoritative (flush() brings it
     // to the host).
-    std::vector<size_t> sample(StateVector& sv, const double* uniforms, size_t shots);
-    size_t measure(StateVector& sv, double u);
+    bool sample(StateVector& sv, const double* uniforms, size_t shots, std::vector<size_t>& out);
+    bool measure(StateVector& sv, double u, size_t& out);
 
 private:
     void ensureOnDevice(StateVector& sv);

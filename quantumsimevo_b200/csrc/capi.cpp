@@ -337,7 +337,7 @@ int qse_state_upload(qse_state* st, const double* host)
     need(st != nullptr && host != nullptr, QSE_ERR_INVALID, "null argument");
     bind_device(st->ctx);
     for (uint32_t q = 0; q < 64; ++q) st->perm[q] = q;
-    st->lazy_zero = false;
+    st->lazy_basis = false;
     st->touch();
     QSE_CUDA(cudaMemcpyAsync(st->amp, host, st->size() * 16, cudaMemcpyHostToDevice, st->ctx->stream));
     QSE_CUDA(cudaStreamSynchronize(st->ctx->stream));

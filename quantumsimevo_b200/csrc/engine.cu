@@ -182,7 +182,7 @@ plan::Plan plan_for(qse_state* st, const std::vector<plan::Gate>& gates, plan::O
     if (!use_jit) return pl;
     srcs.reserve(pl.passes.size());
     for (size_t i = 0; i < pl.passes.size(); ++i)
-        srcs.push_back(jit::generate(pl.passes[i], ns, i == 0 && ns == 1 && st->lazy_zero));
+        srcs.push_back(jit::generate(pl.passes[i], ns, i == 0 && ns == 1 && st->lazy_basis));
     if (st->n >= kJitAlwaysQubits || jit::count_uncached(srcs) <= kJitMaxNewKernels) return pl;
     use_jit = false;
     srcs.clear();
@@ -225,7 +225,7 @@ struct PassRunner {
             return;
         }
         cudaEvent_t stop = tile::pass_timer_begin(ctx);
-        jit::launch(ctx, *ks[i], srcs[i], st->n, kq[i], a.psi, lam, a.terms, a.groups, part);
+        jit::launch(ctx, *ks[i], srcs[i], st->n, kq[i], a.psi, lam, a.terms, a.groups, part, st->lazy_index);
         tile::pass_timer_end(ctx, stop);
         count_launch(ctx);
     }
@@ -297,7 +297,7 @@ void execute_program(qse_state* st, const qse_op* ops, size_t nops, const double
         run_noise(st, noise, ops, nops, inj, ninj, stats);
     }
     uint64_t passes = 0;
-    if (!ctx->fusion || st->n < 4 || !ctx->jit) materialize(st);  // only JIT passes start from a lazy |0..0>
+    if (!ctx->fusion || st->n < 4 || !ctx->jit) materialize(st);  // only JIT passes start from a lazy basis state
     if (!ctx->fusion || st->n < 4) {
         for (const plan::Gate& g : gates) apply_plain(st, g);
         passes = gates.size();
@@ -315,7 +315,7 @@ void execute_program(qse_state* st, const qse_op* ops, size_t nops, const double
         Uploaded up = upload_plan(ctx, pl);
         PassRunner runner(st, pl, up, 1, 4, use_jit, std::move(srcs));
         for (size_t i = 0; i < up.args.size(); ++i) runner.run(i, nullptr, nullptr);
-        if (!up.args.empty()) st->lazy_zero = false;  // the first pass wrote every amplitude
+        if (!up.args.empty()) st->lazy_basis = false;  // the first pass wrote every amplitude
         for (uint32_t q = 0; q < st->n; ++q) st->perm[q] = pl.perm_final[q];
         passes = pl.passes.size();
     }

@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(kBlock) k_swap(double2* __restrict__ a, uint64
     }
 }
 
-__global__ void k_set_first(double2* a) { a[0] = make_double2(1.0, 0.0); }
+__global__ void k_set_one(double2* a, uint64_t i) { a[i] = make_double2(1.0, 0.0); }
 
 // index of the j-th amplitude with physical bit b equal to v (j < 2^(n-1))
 __device__ __forceinline__ uint64_t with_bit(uint64_t j, uint32_t b, uint64_t v)
@@ -371,13 +371,31 @@ void launch_swap(qse_state* st, uint32_t q0, uint32_t q1)
 void mark_zero(qse_state* st)
 {
     for (uint32_t q = 0; q < 64; ++q) st->perm[q] = q;
-    st->lazy_zero = true;
+    mark_basis(st, 0);
+}
+
+void mark_basis(qse_state* st, uint64_t phys_index)
+{
+    st->lazy_basis = true;
+    st->lazy_index = phys_index;
     st->touch();
 }
 
+namespace {
+void write_basis_state(qse_state* st, uint64_t phys_index)
+{
+    st->lazy_basis = false;
+    st->touch();
+    QSE_CUDA(cudaMemsetAsync(st->amp, 0, st->size() * 16, st->ctx->stream));
+    k_set_one<<<1, 1, 0, st->ctx->stream>>>(reinterpret_cast<double2*>(st->amp), phys_index);
+    QSE_CUDA(cudaGetLastError());
+    count_launch(st->ctx);
+}
+}  // namespace
+
 void materialize(qse_state* st)
 {
-    if (st->lazy_zero) launch_init_zero_state(st);
+    if (st->lazy_basis) write_basis_state(st, st->lazy_index);
 }
 
 // StateVector::measureQubit / resetQubit (StateVector.cpp:158-221) with the
@@ -418,15 +436,7 @@ int measure_or_reset_qubit(qse_state* st, uint32_t q, double u, bool reset, doub
     return outcome;
 }
 
-void launch_init_zero_state(qse_state* st)
-{
-    st->lazy_zero = false;
-    st->touch();
-    QSE_CUDA(cudaMemsetAsync(st->amp, 0, st->size() * 16, st->ctx->stream));
-    k_set_first<<<1, 1, 0, st->ctx->stream>>>(reinterpret_cast<double2*>(st->amp));
-    QSE_CUDA(cudaGetLastError());
-    count_launch(st->ctx);
-}
+void launch_init_zero_state(qse_state* st) { write_basis_state(st, 0); }
 
 void scale_state(qse_state* st, double s)
 {

@@ -94,7 +94,8 @@ struct Gen {
     int thr[16];
     int nthr;
 
-    bool zero_in = false;   // generate |0..0> instead of loading (ns == 1)
+    bool zero_in = false;   // generate the basis state |bi> instead of loading (ns == 1)
+    int basis_slot = -1;    // prm slot of bi (set per launch)
     bool xb_used = false;   // the exchange buffer holds data some thread may still read
 
     Gen(const plan::PassProgram& p, int nstates, bool zero_input) : P(p), ns(nstates), zero_in(zero_input && nstates == 1)
@@ -418,12 +419,15 @@ struct Gen {
             if ((P.outer_mask >> q) & 1) o << " ob |= (c & 1ull) << " << q << "; c >>= 1;";
         o << " (void)c; }\n";
         if (zero_in) {
-            // |0..0> input: only the tile holding index 0 has a nonzero amplitude;
-            // every gate is linear, so every other tile's output is zero
-            // zeros stored in tile-local order m = tid + j*T (the tile always holds
-            // physical qubits 0..2, so consecutive threads write consecutive amplitudes)
+            // basis-state input |bi> (bi: physical index, from the parameter block so
+            // one kernel serves every index): only the tile holding bi has a nonzero
+            // amplitude; every gate is linear, so every other tile's output is zero,
+            // stored in tile-local order m = tid + j*T (the tile always holds physical
+            // qubits 0..2, so consecutive threads write consecutive amplitudes)
+            basis_slot = int(push(0.0));
+            o << "  const u64 bi = (u64)P.v[" << basis_slot << "];\n";
             const uint32_t lt = uint32_t(__builtin_ctz(T));
-            o << "  if (ob != 0ull) {\n    const u64 gz = ob";
+            o << "  if (ob != (bi & " << hex(P.outer_mask) << ")) {\n    const u64 gz = ob";
             for (uint32_t b = 0; b < lt; ++b)
                 o << " | ((u64)((tid >> " << b << ") & 1u) << " << int(P.tile_phys[b]) << ")";
             o << ";\n";
@@ -450,10 +454,20 @@ struct Gen {
         }
         // prologue: per-CTA diagonal group values, then the lane tables
         if (ng) {
+            // the pass's terms are first copied into the exchange buffer (unused until
+            // the first layout exchange, which follows the prologue's barrier) by every
+            // thread at once, so the per-group sums read shared memory instead of
+            // issuing one dependent global load per term
+            const size_t nterms = P.terms.size();
+            const bool stage = nterms > 0 && nterms <= tsize;
+            if (stage)
+                o << "  TermRec* ts = reinterpret_cast<TermRec*>(xb);\n"
+                  << "  for (u32 i = tid; i < " << nterms << "u; i += " << T << "u) ts[i] = terms[i];\n"
+                  << "  __syncthreads();\n";
             o << "  for (u32 g = tid; g < " << ng << "u; g += " << T << "u) {\n"
               << "    const GroupRec gr = groups[g]; double th = 0.0;\n"
-              << "    for (u32 i = 0; i < gr.count; ++i) { const TermRec t = terms[gr.first + i];"
-                 " if ((ob & t.ocond) == t.ocond) th += t.theta; }\n"
+              << "    for (u32 i = 0; i < gr.count; ++i) { const TermRec t = " << (stage ? "ts" : "terms")
+              << "[gr.first + i]; if ((ob & t.ocond) == t.ocond) th += t.theta; }\n"
               << "    gv[g] = gr.direct ? expi(th) : make_double2(th, 0.0);\n  }\n";
         }
         if (ntab) o << "  __syncthreads();\n" << tabs.str();
@@ -461,7 +475,7 @@ struct Gen {
         o << "  __syncthreads();\n";
         if (zero_in)
             for (uint32_t j = 0; j < R; ++j)
-                o << "  a0[" << j << "] = make_double2((gb | " << hex(reg_off(j)) << ") == 0ull ? 1.0 : 0.0, 0.0);\n";
+                o << "  a0[" << j << "] = make_double2((gb | " << hex(reg_off(j)) << ") == bi ? 1.0 : 0.0, 0.0);\n";
         std::swap(o, head);
 
         std::ostringstream src;
@@ -643,12 +657,13 @@ bool available(std::string* why)
     return nv.ok;
 }
 
-Source generate(const plan::PassProgram& p, int nstates, bool zero_input)
+Source generate(const plan::PassProgram& p, int nstates, bool basis_input)
 {
-    Gen g(p, nstates, zero_input);
+    Gen g(p, nstates, basis_input);
     Source s;
     s.code = g.run();
     s.prm = std::move(g.prm);
+    s.basis_slot = g.basis_slot;
     s.threads = g.T;
     s.smem = (size_t(1) << p.k) * 16 + p.groups.size() * 16 + size_t(g.ntab) * 32 * 16 +
              (nstates == 2 ? p.slot_src.size() * g.NW * 8 : 0);
@@ -707,7 +722,7 @@ std::vector<std::shared_ptr<Kernel>> get_kernels(const std::vector<const Source*
 }
 
 void launch(qse_ctx* ctx, Kernel& k, const Source& s, uint32_t n, uint32_t kq, void* psi, void* lam,
-            const void* terms, const void* groups, double* slot_partial)
+            const void* terms, const void* groups, double* slot_partial, uint64_t basis_index)
 {
     if (s.smem > ctx->smem_optin) fail(QSE_ERR_SIZE, "pass needs more shared memory than the device offers");
     if (s.smem > k.smem_set) {
@@ -716,6 +731,7 @@ void launch(qse_ctx* ctx, Kernel& k, const Source& s, uint32_t n, uint32_t kq, v
         k.smem_set = s.smem;
     }
     std::vector<double> prm = s.prm;
+    if (s.basis_slot >= 0) prm[size_t(s.basis_slot)] = double(basis_index);   // exact below 2^53
     if (prm.empty()) prm.push_back(0.0);
     void* args[] = {&psi, &lam, const_cast<const void**>(&terms), const_cast<const void**>(&groups), &slot_partial,
                     prm.data()};

@@ -19,6 +19,7 @@ struct Source {
     std::vector<double> prm;  // the kernel's parameter block (angles, matrices, scales)
     uint32_t threads = 0;
     size_t smem = 0;
+    int basis_slot = -1;      // basis-input passes: the prm slot that takes the basis index
 };
 
 struct Kernel {
@@ -31,15 +32,17 @@ struct Kernel {
 bool available(std::string* why);
 // compiles one source without loading it (no GPU needed); returns the cubin size
 size_t compile_only(const Source& s);
-// zero_input: the state is |0..0> (not in memory); the pass generates its
-// input amplitudes instead of loading them (forward passes only)
-Source generate(const plan::PassProgram& p, int nstates, bool zero_input = false);
+// basis_input: the state is a basis state |i> that is not in memory; the pass
+// generates its input amplitudes instead of loading them (forward passes only;
+// i is set per launch, so one kernel serves every i)
+Source generate(const plan::PassProgram& p, int nstates, bool basis_input = false);
 // distinct sources among srcs that are not compiled yet
 size_t count_uncached(const std::vector<Source>& srcs);
 // compiled kernels for every source (cached by source text; missing ones are compiled in parallel)
 std::vector<std::shared_ptr<Kernel>> get_kernels(const std::vector<const Source*>& srcs);
+// basis_index: the physical index of a basis-input pass's input state (ignored otherwise)
 void launch(qse_ctx* ctx, Kernel& k, const Source& s, uint32_t n, uint32_t kq, void* psi, void* lam,
-            const void* terms, const void* groups, double* slot_partial);
+            const void* terms, const void* groups, double* slot_partial, uint64_t basis_index = 0);
 
 }  // namespace jit
 }  // namespace qse

@@ -80,9 +80,10 @@ struct qse_state {
     double* aux = nullptr;       // second state (adjoint |lambda>), allocated on first use
     uint32_t perm[64];           // logical qubit -> physical bit
     uint64_t version = 0;        // bumped by every call that writes the amplitudes
-    bool lazy_zero = false;      // the state is |0..0> (identity qubit map) but the array has
-                                 // not been written: the next fused execute generates it in its
-                                 // first pass, every other reader calls materialize() first
+    bool lazy_basis = false;     // the state is the basis state |lazy_index> (a physical index)
+    uint64_t lazy_index = 0;     // but the array has not been written: the next fused execute
+                                 // generates it in its first pass, every other reader calls
+                                 // materialize() first (reset: |0..0>; measure: the outcome)
     // exact cumulative probabilities (sample.cu), valid while cdf_version == version
     qse::DevBuf cdf;
     uint64_t cdf_version = ~uint64_t(0);
@@ -128,11 +129,12 @@ void launch_ry(qse_state* st, uint32_t q, double c, double s);
 void launch_rz(qse_state* st, uint32_t q, double c0, double s0, double c1, double s1);
 void launch_cnot(qse_state* st, uint32_t c, uint32_t t);
 void launch_swap(qse_state* st, uint32_t q0, uint32_t q1);
-void launch_init_zero_state(qse_state* st);
+void launch_init_zero_state(qse_state* st);                          // write |0..0> now
+void mark_basis(qse_state* st, uint64_t phys_index);                 // lazy |phys_index>
 void mark_zero(qse_state* st);       // reset without writing: lazy |0..0>
 // StateVector::measureQubit (reset = false) / resetQubit (reset = true), draw u injected
 int measure_or_reset_qubit(qse_state* st, uint32_t qubit, double u, bool reset, double* prob1);
-void materialize(qse_state* st);     // write a lazy |0..0> into the array (no-op otherwise)
+void materialize(qse_state* st);     // write a lazy basis state into the array (no-op otherwise)
 void launch_pauli_frame(qse_state* st, const int32_t* d_counts);      // Noise::applyPauliNoise
 void permute_to_logical(qse_state* st, double* dst_device);           // gather into logical order
 void scale_state(qse_state* st, double s);

@@ -1119,12 +1119,6 @@ CdfView build_cdf(qse_state* st)
     return v;
 }
 
-__global__ void k_collapse(double2* amp, uint64_t size, uint64_t phys)
-{
-    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < size; i += uint64_t(gridDim.x) * blockDim.x)
-        amp[i] = make_double2(i == phys ? 1.0 : 0.0, 0.0);
-}
-
 }  // namespace
 
 void sample(qse_state* st, const double* u_host, size_t nshots, uint64_t seed, uint64_t* out_host)
@@ -1163,17 +1157,11 @@ uint64_t measure(qse_state* st, double u)
 {
     uint64_t idx = 0;
     sample(st, &u, 1, 0, &idx);
-    // StateVector.cpp:142-149: every amplitude 0, the outcome 1 (no phase kept)
+    // StateVector.cpp:142-149: every amplitude 0, the outcome 1 (no phase kept).
+    // Recorded, not written: the next fused execute generates the basis state in
+    // its first pass, a reset discards it, any other reader writes it first.
     uint64_t L = idx < st->size() ? idx : 0;
-    uint64_t P = logical_to_physical_index(st, L);
-    qse_ctx* ctx = st->ctx;
-    uint64_t size = st->size();
-    unsigned grid = unsigned(std::min<uint64_t>((size + 255) / 256, uint64_t(ctx->num_sms) * 32));
-    k_collapse<<<grid, 256, 0, ctx->stream>>>(reinterpret_cast<double2*>(st->amp), size, P);
-    st->touch();
-    QSE_CUDA(cudaGetLastError());
-    count_launch(ctx);
-    QSE_CUDA(cudaStreamSynchronize(ctx->stream));
+    mark_basis(st, logical_to_physical_index(st, L));
     return L;
 }
 

@@ -234,6 +234,10 @@ def load_reference(gpu=False):
         "ref_statevector_get": ([_vp, _vp], None),
         "ref_statevector_set": ([_vp, _vp], None),
         "ref_statevector_measure_qubit": ([_vp, C.c_uint], C.c_int),
+        "ref_statevector_measure": ([_vp], _u64),
+        "ref_statevector_sample": ([_vp, C.c_int, _pu64], None),
+        "ref_statevector_reset": ([_vp], None),
+        "ref_device_synchronize": ([], C.c_int),
         "ref_statevector_reset_qubit": ([_vp, C.c_uint], None),
         "ref_playground_build": ([_vp, C.c_int, C.c_int, C.c_int], C.c_int),
         "ref_tsp_ising": ([_pd, C.c_uint, _d, _d, C.c_int, C.c_int, _pd, C.POINTER(C.c_uint), _pd, C.c_uint,

@@ -139,6 +139,48 @@ def test_reset_then_every_reader_sees_zero_state(dev):
     assert np.array_equal(st.download(), zero)
 
 
+def test_measure_then_every_reader_sees_the_basis_state(dev):
+    """measure() records the outcome's basis state without writing the array:
+    the next fused execute generates it in its first pass (kernel shared with
+    reset, the index in its parameter block), every other reader writes it
+    first, and a reset discards it.  Relabelled qubits (swaps before the measure)
+    included; states of 13 and 23 qubits (one tile / many tiles per pass)."""
+    for n in (13, 23):
+        pre = np.concatenate([W.random_circuit(n, 60, 31 + n), W.to_array(W.qft_ops(n))])
+        ops = W.random_circuit(n, 80, 41 + n)
+        st = StateVector(n, dev)
+
+        def measured(u):
+            L.check(L.lib.qse_state_reset(st.handle))
+            L.check(L.lib.qse_execute(st.handle, L.dptr(pre), len(pre), None, 0, None, None, 0, None))
+            idx = C.c_uint64()
+            L.check(L.lib.qse_measure(st.handle, u, C.byref(idx)))
+            basis = np.zeros(1 << n, dtype=np.complex128)
+            basis[int(idx.value)] = 1.0
+            return basis
+
+        for u in (0.1, 0.77):
+            basis = measured(u)
+            assert np.array_equal(st.download(), basis)
+            basis = measured(u)
+            L.check(L.lib.qse_execute(st.handle, L.dptr(ops), len(ops), None, 0, None, None, 0, None))
+            assert np.max(np.abs(st.download() - O.run_on(basis, n, ops))) <= TOL
+            basis = measured(u)
+            dev.set_fusion(False)
+            L.check(L.lib.qse_execute(st.handle, L.dptr(ops), len(ops), None, 0, None, None, 0, None))
+            dev.set_fusion(True, 12, 0)
+            assert np.max(np.abs(st.download() - O.run_on(basis, n, ops))) <= TOL
+            basis = measured(u)
+            uu = np.linspace(0.01, 0.99, 8)
+            out = np.zeros(8, dtype=np.uint64)
+            L.check(L.lib.qse_sample(st.handle, uu.ctypes.data_as(L._pd), 8, 0, out.ctypes.data_as(L._pu64)))
+            assert np.all(out == np.flatnonzero(basis)[0])
+            measured(u)
+            L.check(L.lib.qse_state_reset(st.handle))
+            L.check(L.lib.qse_execute(st.handle, L.dptr(ops), len(ops), None, 0, None, None, 0, None))
+            assert np.max(np.abs(st.download() - O.run(n, ops))) <= TOL
+
+
 def test_execute_twice_and_swap_relabel(dev):
     # Circuit::execute does not clear its queue: a second execute applies it again
     n = 11
