@@ -50,6 +50,9 @@
 #endif
 
 static int g_backend = 0;
+#ifdef QSE_REF_WITH_GPU
+static CircuitUnitaryOperationB200* g_last_b200 = nullptr;   // the newest adapter the factory made
+#endif
 
 std::unique_ptr<ICircuitUnitaryOperation> CircuitUnitaryOperationFactory::create(size_t numQubits)
 {
@@ -58,7 +61,11 @@ std::unique_ptr<ICircuitUnitaryOperation> CircuitUnitaryOperationFactory::create
     case 1: return std::make_unique<CircuitUnitaryOperationAVX>();
 #ifdef QSE_REF_WITH_GPU
     case 2: return std::make_unique<CircuitUnitaryOperationGPU>();
-    case 3: return std::make_unique<CircuitUnitaryOperationB200>();
+    case 3: {
+        auto p = std::make_unique<CircuitUnitaryOperationB200>();
+        g_last_b200 = p.get();
+        return p;
+    }
 #endif
     default: return std::make_unique<CircuitUnitaryOperation>();
     }
@@ -295,6 +302,17 @@ int ref_b200_sample(void* be, void* svp, const double* u, size_t shots, uint64_t
 #else
     (void)be; (void)svp; (void)u; (void)shots; (void)out;
     return -1;
+#endif
+}
+
+// Kernels launched so far by the newest adapter the factory made (tells the
+// fused path, a few passes, from one kernel per gate); 0 without one.
+uint64_t ref_b200_kernel_launches(void)
+{
+#ifdef QSE_REF_WITH_GPU
+    return g_last_b200 ? qse_ctx_kernel_launches(g_last_b200->context()) : 0;
+#else
+    return 0;
 #endif
 }
 

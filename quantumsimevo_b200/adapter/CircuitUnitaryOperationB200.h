@@ -61,6 +61,9 @@ public:
     bool sample(StateVector& sv, const double* uniforms, size_t shots, std::vector<size_t>& out);
     bool measure(StateVector& sv, double u, size_t& out);
 
+    // the C-ABI context (device + stream) this backend runs on
+    qse_ctx* context() const { return ctx_; }
+
 private:
     void ensureOnDevice(StateVector& sv);
     void check(int status, const char* what) const;

@@ -13,6 +13,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_PATH = os.path.join(ROOT, "oracle", "libqse_oracle.so")
 REF_CPU_PATH = os.path.join(ROOT, "oracle", "_ref", "libqse_ref_cpu.so")
 REF_GPU_PATH = os.path.join(ROOT, "oracle", "_ref", "libqse_ref_gpu.so")
+REF_PATCHED_PATH = os.path.join(ROOT, "oracle", "_ref", "libqse_ref_patched.so")
 
 _vp, _u32, _u64, _sz, _d = C.c_void_p, C.c_uint32, C.c_uint64, C.c_size_t, C.c_double
 _pd, _pu64 = C.POINTER(C.c_double), C.POINTER(C.c_uint64)
@@ -203,8 +204,11 @@ def philox_pair(seed, counter):
 
 
 # ---------------- compiled reference (oracle/_ref) ----------------
-def load_reference(gpu=False):
-    path = REF_GPU_PATH if gpu else REF_CPU_PATH
+def load_reference(gpu=False, patched=False):
+    """The reference compiled into oracle/_ref: CPU backends, or (gpu) also its
+    CUDA backend and this project's adapter, or (patched) the GPU build over a
+    copy of the reference tree with the optional Circuit -> backend hooks."""
+    path = REF_PATCHED_PATH if patched else REF_GPU_PATH if gpu else REF_CPU_PATH
     if not os.path.exists(path):
         return None
     lib = C.CDLL(path)
@@ -243,9 +247,12 @@ def load_reference(gpu=False):
         "ref_tsp_ising": ([_pd, C.c_uint, _d, _d, C.c_int, C.c_int, _pd, C.POINTER(C.c_uint), _pd, C.c_uint,
                            C.POINTER(C.c_uint)], C.c_int),
     }
-    if gpu:
+    if gpu or patched:
         sigs["ref_b200_sample"] = ([_vp, _vp, _pd, _sz, _pu64], C.c_int)
         sigs["ref_b200_measure"] = ([_vp, _vp, _d, _pu64], C.c_int)
+        sigs["ref_b200_kernel_launches"] = ([], _u64)
+    if patched:
+        sigs["ref_inject_uniforms"] = ([_pd, _sz], None)
     for name, (a, r) in sigs.items():
         f = getattr(lib, name)
         f.argtypes = a

@@ -179,3 +179,55 @@ def test_python_circuit_parameters_expectation_gradient_measure_qubit():
     assert o in (0, 1)
     idx = 1 << 2 | 1 << 6 if o else 0
     assert abs(abs(st[idx]) - 1.0) <= 1e-12
+
+
+@pytest.fixture(scope="module")
+def ref_patched():
+    r = O.load_reference(patched=True)
+    if r is None:
+        pytest.skip("oracle/_ref/libqse_ref_patched.so not built")
+    r.ref_set_quiet(1)
+    return r
+
+
+@pytest.mark.parametrize("n", [5, 12, 16])
+def test_patched_reference_circuit_takes_the_fused_path(ref_patched, n):
+    """The reference's own Circuit compiled over a copy of its tree whose
+    interface declares the optional hooks (oracle/patch_reference.py):
+    Circuit::execute hands the whole queue to CircuitUnitaryOperationB200::
+    executeProgram -> qse_execute (fused passes), and Circuit::sample /
+    Circuit::measure hand their draws to the device sampler.  Against the same
+    Circuit on the scalar backend, whose hooks decline: amplitudes <= 1e-12
+    (SWAP and MCPHASE included); the execute launches a few passes, not one
+    kernel per gate; sample / measure give the oracle's outcomes for the
+    injected draws on the device state."""
+    r = ref_patched
+    ops = W.random_circuit(n, 40 * n, 9100 + n, with_2x2=False)
+    assert np.any(ops["type"] == L.SWAP) and np.any(ops["type"] == L.MCPHASE)
+    want = O.ref_run(r, n, ops, backend=0)
+    assert r.ref_set_backend(3) == 0
+    h = r.ref_circuit_new(n, 0)
+    a = np.ascontiguousarray(ops)
+    assert r.ref_circuit_add_many(h, a.ctypes.data_as(C.c_void_p), len(a)) == 0
+    k0 = r.ref_b200_kernel_launches()
+    r.ref_circuit_execute(h, 0)
+    launches = r.ref_b200_kernel_launches() - k0
+    got = np.empty(1 << n, dtype=np.complex128)
+    r.ref_circuit_state(h, got.ctypes.data_as(C.c_void_p))
+    assert np.max(np.abs(got - want)) <= 1e-12
+    assert launches < len(ops) / 4, (launches, len(ops))
+    u = np.random.default_rng(n).random(2000)
+    r.ref_inject_uniforms(u.ctypes.data_as(O._pd), u.size)
+    out = np.empty(u.size, dtype=np.uint64)
+    r.ref_circuit_sample(h, u.size, out.ctypes.data_as(O._pu64))
+    assert np.array_equal(out, O.sample(got, n, u))
+    um = np.array([0.41421356])
+    r.ref_inject_uniforms(um.ctypes.data_as(O._pd), 1)
+    idx = r.ref_circuit_measure(h)
+    want_idx, collapsed = O.measure(got, n, um[0])
+    assert idx == want_idx
+    after = np.empty(1 << n, dtype=np.complex128)
+    r.ref_circuit_state(h, after.ctypes.data_as(C.c_void_p))
+    assert np.array_equal(after, collapsed)
+    r.ref_circuit_free(h)
+    r.ref_set_backend(0)
