@@ -231,11 +231,16 @@ QSE_API int qse_plan_describe(uint32_t nqubits, const qse_op* ops, size_t nops, 
 
 /* Pass kernels: 1 (default) = each planned pass is specialised into its own
  * kernel and compiled for sm_100a at run time (cached by source); 0 = one
- * generic kernel interprets the pass program. */
+ * generic kernel interprets the pass program; 2 = specialised, and forward
+ * read+write passes over at least 2^10 tiles run as a persistent streamed
+ * kernel (one CTA per SM, tiles arriving in shared memory by bulk async copies
+ * while two thread groups compute). */
 QSE_API int qse_ctx_set_jit(qse_ctx* ctx, int enabled);
 /* Generates and compiles (no GPU needed, nothing loaded) every distinct pass
  * kernel the planner makes for ops: nstates 1 = forward passes, 2 = adjoint
- * reverse passes.  *source_bytes receives the total generated source size. */
+ * reverse passes, 3 = forward passes as streamed kernels where a pass allows
+ * it (qse_ctx_set_jit mode 2).  *source_bytes receives the total generated
+ * source size. */
 QSE_API int qse_plan_compile(uint32_t nqubits, const qse_op* ops, size_t nops, const double* params,
                              size_t nparams, uint32_t tile_qubits, int nstates, size_t* source_bytes);
 

@@ -155,6 +155,9 @@ int qse_ctx_create(int device, qse_ctx** out)
     QSE_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
     ctx->smem_optin = size_t(optin);
     QSE_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    QSE_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&ctx->status_host), 16, cudaHostAllocMapped));
+    *reinterpret_cast<volatile unsigned*>(ctx->status_host) = 0u;
+    QSE_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->status_dev), ctx->status_host, 0));
     QSE_CUDA(cudaEventCreateWithFlags(&ctx->plan_event, cudaEventDisableTiming));
     QSE_CUDA(cudaEventRecord(ctx->plan_event, ctx->stream));
     *out = ctx;
@@ -178,6 +181,7 @@ int qse_ctx_destroy(qse_ctx* ctx)
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->pass_events) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->status_host) cudaFreeHost(ctx->status_host);
     delete ctx;
     QSE_GUARD_END
 }
@@ -188,6 +192,7 @@ int qse_ctx_synchronize(qse_ctx* ctx)
     need(ctx != nullptr, QSE_ERR_INVALID, "null context");
     bind_device(ctx);
     QSE_CUDA(cudaStreamSynchronize(ctx->stream));
+    qse::check_device_status(ctx);
     QSE_GUARD_END
 }
 
@@ -350,6 +355,7 @@ int qse_state_download(qse_state* st, double* host)
     need(st != nullptr && host != nullptr, QSE_ERR_INVALID, "null argument");
     bind_device(st->ctx);
     qse::download_logical(st, host);
+    qse::check_device_status(st->ctx);
     QSE_GUARD_END
 }
 
@@ -360,6 +366,7 @@ int qse_state_download_range(qse_state* st, uint64_t first, uint64_t count, doub
     need(first <= st->size() && count <= st->size() - first, QSE_ERR_INVALID, "range outside the state");
     bind_device(st->ctx);
     qse::download_range(st, first, count, host);
+    qse::check_device_status(st->ctx);
     QSE_GUARD_END
 }
 
@@ -564,7 +571,8 @@ int qse_ctx_set_jit(qse_ctx* ctx, int enabled)
 {
     QSE_GUARD_BEGIN
     need(ctx != nullptr, QSE_ERR_INVALID, "null context");
-    ctx->jit = enabled ? 1 : 0;
+    need(enabled >= 0 && enabled <= 2, QSE_ERR_INVALID, "pass kernel mode must be 0, 1 or 2");
+    ctx->jit = enabled;
     QSE_GUARD_END
 }
 
@@ -574,7 +582,9 @@ int qse_plan_compile(uint32_t nqubits, const qse_op* ops, size_t nops, const dou
     QSE_GUARD_BEGIN
     need(nqubits >= 3 && nqubits <= 40, QSE_ERR_SIZE, "qubit count out of range");
     need(nops == 0 || ops != nullptr, QSE_ERR_INVALID, "null ops");
-    need(nstates == 1 || nstates == 2, QSE_ERR_INVALID, "nstates must be 1 or 2");
+    need(nstates >= 1 && nstates <= 3, QSE_ERR_INVALID, "nstates must be 1, 2 or 3");
+    const bool streamed = nstates == 3;
+    if (streamed) nstates = 1;
     std::vector<qse::plan::Gate> gates;
     for (size_t i = 0; i < nops; ++i) {
         size_t k = nstates == 2 ? nops - 1 - i : i;
@@ -601,7 +611,7 @@ int qse_plan_compile(uint32_t nqubits, const qse_op* ops, size_t nops, const dou
     size_t total = 0;
     std::set<std::string> done;   // identical passes share one kernel, as in execution
     for (const auto& p : pl.passes) {
-        qse::jit::Source s = qse::jit::generate(p, nstates);
+        qse::jit::Source s = qse::jit::generate(p, nstates, false, streamed);
         total += s.code.size();
         if (done.insert(s.code).second) qse::jit::compile_only(s);
     }
@@ -619,6 +629,7 @@ int qse_sample(qse_state* st, const double* uniforms, size_t nshots, uint64_t se
             need(uniforms[i] >= 0.0 && uniforms[i] < 1.0, QSE_ERR_INVALID, "uniforms must lie in [0,1)");
     bind_device(st->ctx);
     qse::sample(st, uniforms, nshots, seed, out_indices);
+    qse::check_device_status(st->ctx);
     QSE_GUARD_END
 }
 
@@ -639,6 +650,7 @@ int qse_measure(qse_state* st, double u, uint64_t* out_index)
     need(u >= 0.0 && u < 1.0, QSE_ERR_INVALID, "u must lie in [0,1)");
     bind_device(st->ctx);
     *out_index = qse::measure(st, u);
+    qse::check_device_status(st->ctx);
     QSE_GUARD_END
 }
 
@@ -678,6 +690,7 @@ int qse_total_probability(qse_state* st, double* total)
     need(st != nullptr && total != nullptr, QSE_ERR_INVALID, "null argument");
     bind_device(st->ctx);
     *total = qse::total_probability(st);
+    qse::check_device_status(st->ctx);
     QSE_GUARD_END
 }
 
@@ -688,6 +701,7 @@ int qse_expectation(qse_state* st, const qse_observable* obs, double* value)
     need(obs->nterms == 0 || (obs->zmask && obs->weight), QSE_ERR_INVALID, "null observable terms");
     bind_device(st->ctx);
     *value = qse::expectation(st, obs);
+    qse::check_device_status(st->ctx);
     QSE_GUARD_END
 }
 

@@ -2,9 +2,11 @@
 // list -> planner -> one tile-kernel launch per pass; noise decisions and the
 // end-of-execute Pauli frame; expectation values and the adjoint sweep.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 
 #include "jit.h"
 #include "planner.h"
@@ -182,7 +184,7 @@ plan::Plan plan_for(qse_state* st, const std::vector<plan::Gate>& gates, plan::O
     if (!use_jit) return pl;
     srcs.reserve(pl.passes.size());
     for (size_t i = 0; i < pl.passes.size(); ++i)
-        srcs.push_back(jit::generate(pl.passes[i], ns, i == 0 && ns == 1 && st->lazy_basis));
+        srcs.push_back(jit::generate(pl.passes[i], ns, i == 0 && ns == 1 && st->lazy_basis, st->ctx->jit == 2));
     if (st->n >= kJitAlwaysQubits || jit::count_uncached(srcs) <= kJitMaxNewKernels) return pl;
     use_jit = false;
     srcs.clear();
@@ -220,14 +222,22 @@ struct PassRunner {
         a.psi = reinterpret_cast<double2*>(st->amp);
         a.lam = lam;
         a.slot_partial = part;
+        // one NVTX range per planned pass (host side, around the launch; free
+        // unless a profiler injects an NVTX handler)
+        char name[64];
+        std::snprintf(name, sizeof(name), "qse pass %zu/%zu %s%s", i + 1, up.args.size(),
+                      ns == 2 ? "adjoint " : "", !jit ? "interpreter" : srcs[i].streamed ? "streamed" : "tile");
+        nvtxRangePushA(name);
         if (!jit) {
             tile::launch_pass(ctx, a, st->n, rb, ns);
+            nvtxRangePop();
             return;
         }
         cudaEvent_t stop = tile::pass_timer_begin(ctx);
         jit::launch(ctx, *ks[i], srcs[i], st->n, kq[i], a.psi, lam, a.terms, a.groups, part, st->lazy_index);
         tile::pass_timer_end(ctx, stop);
         count_launch(ctx);
+        nvtxRangePop();
     }
 };
 

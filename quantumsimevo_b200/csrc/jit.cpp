@@ -97,6 +97,7 @@ struct Gen {
     bool zero_in = false;   // generate the basis state |bi> instead of loading (ns == 1)
     int basis_slot = -1;    // prm slot of bi (set per launch)
     bool xb_used = false;   // the exchange buffer holds data some thread may still read
+    std::string SYNC = "__syncthreads();";   // barrier of the threads that share xb
 
     Gen(const plan::PassProgram& p, int nstates, bool zero_input) : P(p), ns(nstates), zero_in(zero_input && nstates == 1)
     {
@@ -485,10 +486,155 @@ struct Gen {
         const uint32_t min_blocks = std::max(1u, std::min(8u, 65536u / (T * 128u)));
         src << "extern \"C\" __global__ void __launch_bounds__(" << T << ", " << min_blocks << ") qse_pass("
             << "double2* __restrict__ psi, double2* __restrict__ lam, const TermRec* __restrict__ terms, "
-            << "const GroupRec* __restrict__ groups, double* __restrict__ slot_partial, const __grid_constant__ Prm P)\n{\n"
-            << "  (void)lam; (void)terms; (void)groups; (void)slot_partial;\n"
+            << "const GroupRec* __restrict__ groups, double* __restrict__ slot_partial, u32* __restrict__ status, "
+            << "const __grid_constant__ Prm P)\n{\n"
+            << "  (void)lam; (void)terms; (void)groups; (void)slot_partial; (void)status;\n"
             << head.str() << ops_txt << "}\n";
         return src.str();
+    }
+
+    // ---- streamed pass (forward passes on large states) ----
+    // One persistent CTA per SM with two compute groups of T threads that take
+    // alternate tiles.  Tiles arrive in a ring of three shared-memory slots by
+    // bulk async copies (one per contiguous piece of 2^c amplitudes, completion
+    // counted on the slot's mbarrier).  A group waits for its slot, loads its
+    // registers from it, runs the pass with the slot as its exchange buffer
+    // (group-local named barriers), stores straight to global memory, and then
+    // itself issues the copies of the tile three ahead into the slot it just
+    // freed -- a tile the other group takes next -- so the loads of upcoming
+    // tiles run while both groups compute.  Every wait is bounded: a wait that
+    // gives up writes a nonzero code to *status (mapped host memory, plain stores) and the group leaves its loop (group-
+    // uniformly); before the CTA exits, thread 0 waits (bounded) for every copy
+    // it knows was issued.
+    static constexpr uint32_t kWaitLimit = 1u << 24;
+
+    static uint32_t contiguous_low_bits(const plan::PassProgram& p)
+    {
+        uint32_t c = 0;
+        while (c < p.k && p.tile_phys[c] == c) ++c;
+        return c;
+    }
+
+    size_t streamed_smem() const
+    {
+        const size_t tsize = size_t(1) << P.k;
+        return 3 * tsize * 16 + 64 + P.terms.size() * 16 + 2 * (P.groups.size() + 32 * size_t(ntab)) * 16;
+    }
+
+    std::string run_streamed()
+    {
+        const uint32_t tsize = 1u << P.k;
+        const uint32_t ng = uint32_t(P.groups.size());
+        const uint32_t nt = uint32_t(P.terms.size());
+        const uint32_t c = contiguous_low_bits(P);
+        const uint32_t npieces = 1u << (P.k - c), piece = 1u << c;
+        const uint32_t nth = 2 * T;
+        const uint32_t lt = uint32_t(__builtin_ctz(T));
+        SYNC = "group_sync(1u + grp, " + std::to_string(T) + "u);";
+        xb_used = true;   // the registers are loaded from the slot the first exchange writes
+
+        set_layout(P.layouts[P.layout0]);
+        std::ostringstream body;
+        std::swap(o, body);
+        if (!P.acc_mul) emit_acc_decls();
+        for (const plan::KOp& op : P.ops) emit_op(op);
+        flush_run();
+        for (uint32_t j = 0; j < R; ++j) o << "      psi[gb + " << hex(reg_off(j)) << "] = a0[" << j << "];\n";
+        std::swap(o, body);
+        const std::string ops_txt = body.str();
+        set_layout(P.layouts[P.layout0]);
+        const uint32_t gstride = ng + 32 * ntab;
+
+        std::string deposit = "u64 ob = 0; { u64 cc = tile;";
+        for (uint32_t q = 0; q < 64; ++q)
+            if ((P.outer_mask >> q) & 1) deposit += " ob |= (cc & 1ull) << " + std::to_string(q) + "; cc >>= 1;";
+        deposit += " (void)cc; }";
+        std::string scatter = "0ull";
+        for (uint32_t b = c; b < P.k; ++b)
+            scatter += " | ((u64)((p >> " + std::to_string(b - c) + ") & 1u) << " + std::to_string(P.tile_phys[b]) + ")";
+        std::string lbase = "0u";
+        for (int t = 0; t < nthr; ++t)
+            lbase += " | (((tid >> " + std::to_string(t) + ") & 1u) << " + std::to_string(thr[t]) + ")";
+        const uint64_t ntiles = uint64_t(1) << __builtin_popcountll(P.outer_mask);
+        const std::string NT = std::to_string(ntiles) + "ull";
+        const std::string LIM = std::to_string(kWaitLimit) + "u";
+
+        std::ostringstream s;
+        s << kPrelude << "\n";
+        s << "struct Prm { double v[" << std::max<size_t>(1, prm.size()) << "]; };\n";
+        // the copies of one tile: lane 0 announces the bytes, the warp's lanes issue the pieces
+        s << "__device__ __forceinline__ void fill(double2* __restrict__ psi, double2* sm, u64* bar, u32* nfill, u64 tile, "
+             "u32 s, u32 lane)\n{\n"
+          << "  if (lane == 0u) { mbar_expect_tx(bar + s, " << tsize * 16 << "u); nfill[s] += 1u; }\n"
+          << "  __syncwarp();\n"
+          << "  " << deposit << "\n"
+          << "  double2* const dst = sm + s * " << tsize << "u;\n"
+          << "  for (u32 p = lane; p < " << npieces << "u; p += 32u)\n"
+          << "    bulk_g2s(dst + p * " << piece << "u, psi + (ob | " << scatter << "), " << piece * 16 << "u, bar + s);\n"
+          << "}\n";
+        s << "extern \"C\" __global__ void __launch_bounds__(" << nth << ", 1) qse_pass("
+          << "double2* __restrict__ psi, double2* __restrict__ lam, const TermRec* __restrict__ terms, "
+          << "const GroupRec* __restrict__ groups, double* __restrict__ slot_partial, u32* __restrict__ status, "
+          << "const __grid_constant__ Prm P)\n{\n"
+          << "  (void)lam; (void)slot_partial;\n"
+          << "  extern __shared__ __align__(128) double2 sm[];\n"
+          << "  u64* const bar = reinterpret_cast<u64*>(sm + " << 3 * tsize << ");   // one per slot\n"
+          << "  u32* const nfill = reinterpret_cast<u32*>(bar + 4);                   // copies issued per slot\n"
+          << "  TermRec* const ts = reinterpret_cast<TermRec*>(bar + 8);\n"
+          << "  double2* const gscr = reinterpret_cast<double2*>(ts + " << nt << ");\n"
+          << "  const u32 tx = threadIdx.x, grp = tx >> " << lt << ", tid = tx & " << (T - 1) << "u;\n"
+          << "  if (tx == 0u) {\n"
+          << "    for (u32 i = 0; i < 3u; ++i) { mbar_init(bar + i, 1u); nfill[i] = 0u; }\n"
+          << "    mbar_fence_init();\n"
+          << "  }\n"
+          << "  __syncthreads();\n"
+          << "  if (tx < 32u)\n"
+          << "    for (u32 i = 0; i < 3u; ++i)\n"
+          << "      if (blockIdx.x + (u64)i * gridDim.x < " << NT << ") fill(psi, sm, bar, nfill, blockIdx.x + (u64)i * gridDim.x, i, tx);\n"
+          << "  for (u32 i = tx; i < " << nt << "u; i += " << nth << "u) ts[i] = terms[i];\n"
+          << "  __syncthreads();\n"
+          << "  double2* const gv = gscr + grp * " << gstride << "u; (void)gv;\n"
+          << "  double2* const tb = gv + " << ng << "; (void)tb;\n"
+          << "  u32 it = grp;\n"
+          << "  for (u64 tile = blockIdx.x + (u64)grp * gridDim.x; tile < " << NT << "; tile += 2ull * gridDim.x, it += 2u) {\n"
+          << "    const u32 s = it % 3u, use = it / 3u;\n"
+          << "    double2* const xb = sm + s * " << tsize << "u;\n"
+          << "    " << deposit << "\n";
+        if (ng) {
+            s << "    for (u32 g = tid; g < " << ng << "u; g += " << T << "u) {\n"
+              << "      const GroupRec gr = groups[g]; double th = 0.0;\n"
+              << "      for (u32 i = 0; i < gr.count; ++i) { const TermRec t = ts[gr.first + i];"
+                 " if ((ob & t.ocond) == t.ocond) th += t.theta; }\n"
+              << "      gv[g] = gr.direct ? expi(th) : make_double2(th, 0.0);\n    }\n";
+            s << "    " << SYNC << "\n";
+            if (ntab) s << tabs.str() << "    " << SYNC << "\n";
+        }
+        s << "    if (!group_all(1u + grp, " << T << "u, mbar_wait(bar + s, use & 1u, " << LIM << "))) {"
+             " if (tid == 0u) *(volatile u32*)status = 1u; break; }\n"
+          << "    {\n"
+          << "      u64 gb = " << gbase_expr() << ";\n"
+          << "      const u32 lb = " << lbase << ";\n"
+          << "      double2 a0[" << R << "];\n";
+        for (uint32_t j = 0; j < R; ++j) {
+            uint32_t loc = 0;
+            for (uint32_t i = 0; i < P.rb; ++i)
+                if ((j >> i) & 1) loc |= 1u << reg[i];
+            s << "      a0[" << j << "] = xb[lb + " << loc << "u];\n";
+        }
+        s << ops_txt
+          << "    }\n"
+          << "    fence_proxy_async();   // this group's shared-memory writes before the copies that reuse the slot\n"
+          << "    " << SYNC << "\n"
+          << "    const u64 next = tile + 3ull * gridDim.x;\n"
+          << "    if (tid < 32u && next < " << NT << ") fill(psi, sm, bar, nfill, next, s, tid);\n"
+          << "  }\n"
+          << "  __syncthreads();\n"
+          << "  // copies a group that gave up did not consume complete before the CTA leaves\n"
+          << "  if (tx == 0u)\n"
+          << "    for (u32 i = 0; i < 3u; ++i)\n"
+          << "      if (nfill[i] != 0u && !mbar_wait(bar + i, (nfill[i] - 1u) & 1u, " << LIM << ")) *(volatile u32*)status = 2u;\n"
+          << "}\n";
+        return s.str();
     }
 
     void emit(const plan::KOp& op)
@@ -574,10 +720,10 @@ struct Gen {
             for (int s = 0; s < ns; ++s) {
                 const char* A = s ? "a1" : "a0";
                 // the first exchange of a pass follows the prologue's barrier: nobody reads xb yet
-                if (xb_used) o << "    __syncthreads();\n";
+                if (xb_used) o << "    " << SYNC << "\n";
                 xb_used = true;
                 for (uint32_t j = 0; j < R; ++j) o << "    xb[sw ^ " << woff[j] << "u] = " << A << "[" << j << "];\n";
-                o << "    __syncthreads();\n";
+                o << "    " << SYNC << "\n";
                 for (uint32_t j = 0; j < R; ++j)
                     o << "    " << A << "[" << j << "] = xb[sr ^ " << slot_off(nl, j) << "u];\n";
             }
@@ -657,8 +803,27 @@ bool available(std::string* why)
     return nv.ok;
 }
 
-Source generate(const plan::PassProgram& p, int nstates, bool basis_input)
+static bool streamable(const plan::PassProgram& p, int nstates, bool basis_input)
 {
+    // forward read+write passes over many tiles whose pieces are at least 128 bytes
+    return nstates == 1 && !basis_input && p.k == 12 && p.rb == 4 && Gen::contiguous_low_bits(p) >= 3 &&
+           __builtin_popcountll(p.outer_mask) >= 10;
+}
+
+Source generate(const plan::PassProgram& p, int nstates, bool basis_input, bool streamed)
+{
+    if (streamed && streamable(p, nstates, basis_input)) {
+        Gen g(p, nstates, false);
+        Source s;
+        s.code = g.run_streamed();
+        if (g.streamed_smem() <= kStreamedSmemMax) {
+            s.prm = std::move(g.prm);
+            s.threads = 2 * g.T;
+            s.smem = g.streamed_smem();
+            s.streamed = true;
+            return s;
+        }
+    }
     Gen g(p, nstates, basis_input);
     Source s;
     s.code = g.run();
@@ -724,6 +889,7 @@ std::vector<std::shared_ptr<Kernel>> get_kernels(const std::vector<const Source*
 void launch(qse_ctx* ctx, Kernel& k, const Source& s, uint32_t n, uint32_t kq, void* psi, void* lam,
             const void* terms, const void* groups, double* slot_partial, uint64_t basis_index)
 {
+    unsigned* status = ctx->status_dev;
     if (s.smem > ctx->smem_optin) fail(QSE_ERR_SIZE, "pass needs more shared memory than the device offers");
     if (s.smem > k.smem_set) {
         QSE_CUDA(cudaFuncSetAttribute(reinterpret_cast<const void*>(k.kern), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -734,8 +900,10 @@ void launch(qse_ctx* ctx, Kernel& k, const Source& s, uint32_t n, uint32_t kq, v
     if (s.basis_slot >= 0) prm[size_t(s.basis_slot)] = double(basis_index);   // exact below 2^53
     if (prm.empty()) prm.push_back(0.0);
     void* args[] = {&psi, &lam, const_cast<const void**>(&terms), const_cast<const void**>(&groups), &slot_partial,
-                    prm.data()};
-    const uint64_t grid = uint64_t(1) << (n - kq);
+                    &status, prm.data()};
+    // streamed passes: one persistent CTA per SM; otherwise one CTA per tile
+    const uint64_t tiles = uint64_t(1) << (n - kq);
+    const uint64_t grid = s.streamed ? std::min<uint64_t>(tiles, uint64_t(ctx->num_sms)) : tiles;
     QSE_CUDA(cudaLaunchKernel(reinterpret_cast<const void*>(k.kern), dim3(unsigned(grid)), dim3(k.threads), args,
                               s.smem, ctx->stream));
 }

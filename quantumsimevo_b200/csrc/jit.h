@@ -20,7 +20,11 @@ struct Source {
     uint32_t threads = 0;
     size_t smem = 0;
     int basis_slot = -1;      // basis-input passes: the prm slot that takes the basis index
+    bool streamed = false;    // persistent streamed kernel (grid = SM count) instead of one CTA per tile
 };
+
+// dynamic shared memory a streamed pass may use (227 KiB per CTA on sm_100)
+constexpr size_t kStreamedSmemMax = 227 * 1024;
 
 struct Kernel {
     cudaLibrary_t lib = nullptr;
@@ -35,7 +39,10 @@ size_t compile_only(const Source& s);
 // basis_input: the state is a basis state |i> that is not in memory; the pass
 // generates its input amplitudes instead of loading them (forward passes only;
 // i is set per launch, so one kernel serves every i)
-Source generate(const plan::PassProgram& p, int nstates, bool basis_input = false);
+// streamed: use the persistent streamed kernel when the pass allows it (forward
+// read+write passes of 12 tile qubits over at least 2^10 tiles, pieces of at
+// least 8 contiguous amplitudes); otherwise one CTA per tile
+Source generate(const plan::PassProgram& p, int nstates, bool basis_input = false, bool streamed = false);
 // distinct sources among srcs that are not compiled yet
 size_t count_uncached(const std::vector<Source>& srcs);
 // compiled kernels for every source (cached by source text; missing ones are compiled in parallel)

@@ -53,11 +53,16 @@ struct qse_ctx {
     cudaStream_t stream = nullptr;
     // planner knobs
     int fusion = 1;
-    int jit = 1;             // specialised NVRTC pass kernels (0: generic interpreter kernel)
+    int jit = 1;             // specialised NVRTC pass kernels (0: generic interpreter kernel,
+                             // 2: specialised, with the streamed persistent kernel where it applies)
     int tile_qubits = 12;
     int max_gates_per_pass = 0;
     int sample_mode = 0;
     uint64_t launches = 0;
+    // device error word of the pass kernels (bounded waits that gave up):
+    // mapped pinned host memory, read on the host after a synchronisation
+    unsigned* status_host = nullptr;
+    unsigned* status_dev = nullptr;
     // scratch shared by the calls on this context (single host thread, like the reference backend)
     qse::DevBuf plan_buf;    // uploaded pass programs
     qse::HostBuf plan_host;  // pinned staging for the pass programs
@@ -115,6 +120,19 @@ namespace qse {
 
 // Launch bookkeeping.
 inline void count_launch(qse_ctx* ctx, uint64_t n = 1) { ctx->launches += n; }
+
+// After a synchronisation of the context's stream: the error word the pass
+// kernels set when one of their bounded waits gave up (then cleared).
+inline void check_device_status(qse_ctx* ctx)
+{
+    if (!ctx->status_host) return;
+    volatile unsigned* s = ctx->status_host;
+    const unsigned v = *s;
+    if (v == 0u) return;
+    *s = 0u;
+    fail(QSE_ERR_TIMEOUT, "a pass kernel's bounded wait gave up (status " + std::to_string(v) +
+                              "); the state's amplitudes are invalid");
+}
 
 // ---- per-gate ("plain method") kernels: gates.cu ----
 void launch_gate2x2(qse_state* st, uint32_t q, const double m[8], uint64_t ctrl_mask);

@@ -892,30 +892,147 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double* __restrict__ pr
     }
 }
 
-// in place: the probabilities of each block are replaced by their exact
-// cumulative sums.  Persistent: blocks blockIdx.x, +gridDim.x, ...; the next
-// block's probabilities stream into the other staging buffer meanwhile, and a
-// block's own buffer then stages its output for the coalesced copy.
-__global__ void __launch_bounds__(kBT, kWriteCTAs) k_cdf_write(const double* __restrict__ cin,
-                                                               double* __restrict__ cdf, uint32_t nb)
+__device__ __forceinline__ uint64_t lower_bound_dev(const double* a, uint64_t n, double target)
+{
+    uint64_t lo = 0, len = n;
+    while (len > 0) {
+        uint64_t half = len >> 1, mid = lo + half;
+        if (a[mid] < target) { lo = mid + 1; len = len - half - 1; }
+        else len = half;
+    }
+    return lo;
+}
+
+// ---- shots against the exact block starts, without a cumulative array ----
+// The cumulative values are never written to memory: each shot's block is
+// found by binary search over the exact block starts cin (a few MB, L2
+// resident), the shots are bucketed by block, and every block that holds a
+// shot rebuilds its exact cumulative values in shared memory (block_exact,
+// the reference's sequential rounding) and answers its shots there.
+
+// target = u * total (StateVector.cpp:100-107's uniform_real_distribution(0, total)),
+// block = first b with cin[b + 1] >= target; targets beyond the total answer size
+__global__ void k_shot_block(const double* __restrict__ cin, uint32_t nb, const double* __restrict__ u,
+                             uint64_t nshots, uint64_t seed, uint64_t size, double* __restrict__ target,
+                             uint32_t* __restrict__ blk, uint32_t* __restrict__ count, uint64_t* __restrict__ out)
+{
+    const double total = cin[nb];
+    for (uint64_t s = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; s < nshots;
+         s += uint64_t(gridDim.x) * blockDim.x) {
+        double us;
+        if (u) us = u[s];
+        else {
+            double u2;
+            philox_uniform_pair(seed, s, kTagSample, us, u2);
+        }
+        const double t = __dadd_rn(__dmul_rn(us, total), 0.0);
+        uint64_t lo = 0, len = nb;
+        while (len > 0) {
+            uint64_t half = len >> 1, mid = lo + half;
+            if (cin[mid + 1] < t) { lo = mid + 1; len = len - half - 1; }
+            else len = half;
+        }
+        target[s] = t;
+        if (lo >= nb) {
+            blk[s] = nb;
+            out[s] = size;   // beyond the end: lower_bound returns size
+        } else {
+            blk[s] = uint32_t(lo);
+            atomicAdd(count + lo, 1u);
+        }
+    }
+}
+
+// one CTA: offset[b] = shots in blocks < b (offset[nb] = all), and the list of
+// blocks holding at least one shot
+constexpr int kOT = 1024;
+__global__ void __launch_bounds__(kOT) k_shot_offsets(const uint32_t* __restrict__ count, uint32_t nb,
+                                                      uint32_t* __restrict__ offset, uint32_t* __restrict__ nonempty,
+                                                      uint32_t* __restrict__ nne)
+{
+    __shared__ uint32_t sa[kOT], sb[kOT];
+    const uint32_t t = threadIdx.x;
+    const uint32_t ch = (nb + kOT - 1) / kOT;
+    const uint32_t lo = min(nb, t * ch), hi = min(nb, lo + ch);
+    uint32_t a = 0, b = 0;
+    for (uint32_t i = lo; i < hi; ++i) {
+        a += count[i];
+        b += count[i] != 0u;
+    }
+    sa[t] = a;
+    sb[t] = b;
+    __syncthreads();
+    for (uint32_t d = 1; d < kOT; d <<= 1) {   // inclusive scan (Hillis-Steele)
+        const uint32_t xa = t >= d ? sa[t - d] : 0u, xb = t >= d ? sb[t - d] : 0u;
+        __syncthreads();
+        sa[t] += xa;
+        sb[t] += xb;
+        __syncthreads();
+    }
+    uint32_t ea = sa[t] - a, eb = sb[t] - b;
+    for (uint32_t i = lo; i < hi; ++i) {
+        offset[i] = ea;
+        ea += count[i];
+        if (count[i]) nonempty[eb++] = i;
+    }
+    if (t == kOT - 1) {
+        offset[nb] = sa[t];
+        *nne = sb[t];
+    }
+}
+
+__global__ void k_shot_scatter(const uint32_t* __restrict__ blk, uint64_t nshots, uint32_t nb,
+                               const uint32_t* __restrict__ offset, uint32_t* __restrict__ cursor,
+                               uint32_t* __restrict__ order)
+{
+    for (uint64_t s = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; s < nshots;
+         s += uint64_t(gridDim.x) * blockDim.x) {
+        const uint32_t b = blk[s];
+        if (b < nb) order[offset[b] + atomicAdd(cursor + b, 1u)] = uint32_t(s);
+    }
+}
+
+// shared memory of k_block_search: two staging buffers + one block's cumulative values
+constexpr size_t kSearchSmem = kStage2 + size_t(kBS) * sizeof(double);
+
+// Persistent over the blocks that hold shots (blockIdx.x, +gridDim.x, ... of
+// the non-empty list): the next block's probabilities stream into the other
+// staging buffer while this block's exact cumulative values are built in
+// shared memory and its shots answered by lower_bound there.
+__global__ void __launch_bounds__(kBT, kWriteCTAs) k_block_search(const double* __restrict__ cin,
+                                                                  const double* __restrict__ prob,
+                                                                  const uint32_t* __restrict__ nonempty,
+                                                                  const uint32_t* __restrict__ nne,
+                                                                  const uint32_t* __restrict__ offset,
+                                                                  const uint32_t* __restrict__ order,
+                                                                  const double* __restrict__ target,
+                                                                  uint64_t* __restrict__ out)
 {
     __shared__ uint64_t sh[160];
     extern __shared__ double stg[];
-    uint32_t b = blockIdx.x;
-    if (b >= nb) return;
-    stage_async(stg, cdf, uint64_t(b) * kBS);
-    for (uint32_t it = 0; b < nb; b += gridDim.x, ++it) {
+    double* const cum = stg + 2 * (kBT * kPad);
+    const uint32_t n = *nne;
+    uint32_t k = blockIdx.x;
+    if (k >= n) return;
+    stage_async(stg, prob, uint64_t(nonempty[k]) * kBS);
+    for (uint32_t it = 0; k < n; k += gridDim.x, ++it) {
         double* cur = stg + (it & 1) * (kBT * kPad);
-        const uint32_t bn = b + gridDim.x;
-        if (bn < nb) {
-            stage_async(stg + ((it + 1) & 1) * (kBT * kPad), cdf, uint64_t(bn) * kBS);
+        const uint32_t kn = k + gridDim.x;
+        if (kn < n) {
+            stage_async(stg + ((it + 1) & 1) * (kBT * kPad), prob, uint64_t(nonempty[kn]) * kBS);
             stage_wait<1>();
         } else {
             stage_wait<0>();
         }
         __syncthreads();
-        block_exact(kBS, cin[b], cdf + uint64_t(b) * kBS, sh, cur);
-        __syncthreads();  // cur is refilled by the next iteration's prefetch
+        const uint32_t b = nonempty[k];
+        block_exact(kBS, cin[b], cum, sh, cur);
+        __syncthreads();
+        for (uint32_t i = offset[b] + threadIdx.x; i < offset[b + 1]; i += kBT) {
+            const uint32_t s = order[i];
+            out[s] = uint64_t(b) * kBS + lower_bound_dev(cum, kBS, target[s]);
+        }
+        __syncthreads();  // cur is refilled by the next iteration's prefetch, cum by the next block
     }
 }
 
@@ -930,17 +1047,6 @@ __global__ void k_cdf_small(const double2* __restrict__ amp, uint64_t size, Perm
     }
     cin[0] = 0.0;
     cin[1] = c;
-}
-
-__device__ __forceinline__ uint64_t lower_bound_dev(const double* a, uint64_t n, double target)
-{
-    uint64_t lo = 0, len = n;
-    while (len > 0) {
-        uint64_t half = len >> 1, mid = lo + half;
-        if (a[mid] < target) { lo = mid + 1; len = len - half - 1; }
-        else len = half;
-    }
-    return lo;
 }
 
 // shots: target = u * total; block by binary search over block starts, then inside the block
@@ -987,7 +1093,10 @@ PermMap make_perm(const qse_state* st)
     return pm;
 }
 
-// Builds the exact cumulative array; returns (cdf, cin, nb, bs) in ctx scratch.
+// The exact sampling tables of a state: states of at least one block (4096
+// amplitudes) keep the probabilities in logical order (cdf) and the exact
+// cumulative value before every block (cin, nb + 1 values); smaller states
+// keep the whole cumulative array (cdf) with cin = {0, total}.
 struct CdfView {
     double* cdf;
     double* cin;
@@ -1051,8 +1160,8 @@ GatherPlan make_gather(const qse_state* st)
     return g;
 }
 
-// Exact cumulative array of the current amplitudes, cached per state until
-// the amplitudes change (sample() followed by measure() builds it once).
+// Exact sampling tables of the current amplitudes, cached per state until the
+// amplitudes change (sample() followed by measure() builds them once).
 CdfView build_cdf(qse_state* st)
 {
     materialize(st);
@@ -1104,12 +1213,10 @@ CdfView build_cdf(qse_state* st)
         k_guess_fin<<<ng, kGT, 0, ctx->stream>>>(bsum, nb, gtot, guess);
         k_cdf_summ<<<nb, kBT, 0, ctx->stream>>>(v.cdf, guess, summ);
         k_cdf_chain<<<1, kBT, 0, ctx->stream>>>(v.cdf, summ, nb, v.cin, reinterpret_cast<uint32_t*>(v.cin + nb + 1));
-        // the attribute belongs to the current device: set on every build
-        QSE_CUDA(cudaFuncSetAttribute(k_cdf_write, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kStage2)));
-        const unsigned pgrid = unsigned(std::min<uint64_t>(nb, uint64_t(ctx->num_sms) * kWriteCTAs));
-        k_cdf_write<<<pgrid, kBT, kStage2, ctx->stream>>>(v.cin, v.cdf, nb);
         QSE_CUDA(cudaGetLastError());
-        count_launch(ctx, 5);
+        count_launch(ctx, 4);
+        // the array keeps the probabilities: shots rebuild the cumulative values
+        // of their blocks in shared memory (sample_blocks)
     }
     st->cdf_values = v.cdf;
     st->cdf_block_start = v.cin;
@@ -1121,22 +1228,68 @@ CdfView build_cdf(qse_state* st)
 
 }  // namespace
 
+namespace {
+size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+// Outcomes of nshots draws (device uniforms d_u, or Philox(seed) when null)
+// into d_out.  `scratch` must hold sample_scratch_bytes(nb, nshots) bytes.
+size_t sample_scratch_bytes(uint32_t nb, size_t nshots)
+{
+    return align16(nshots * 8) + 2 * align16(nshots * 4) + 2 * align16((size_t(nb) + 1) * 4) +
+           align16((size_t(nb) + 2) * 4) + align16(size_t(nb) * 4 + 4) + 16;
+}
+
+void sample_on(qse_state* st, const CdfView& v, const double* d_u, size_t nshots, uint64_t seed, uint64_t* d_out,
+               char* scratch)
+{
+    qse_ctx* ctx = st->ctx;
+    const unsigned grid = unsigned(std::min<uint64_t>((nshots + 255) / 256, uint64_t(ctx->num_sms) * 8));
+    if (st->size() < uint64_t(kBS)) {   // small state: the whole cumulative array
+        k_sample<<<grid, 256, 0, ctx->stream>>>(v.cdf, st->size(), v.cin, v.nb, v.bs, d_u, nshots, seed, d_out,
+                                                make_perm(st));
+        QSE_CUDA(cudaGetLastError());
+        count_launch(ctx);
+        return;
+    }
+    const uint32_t nb = v.nb;
+    char* p = scratch;
+    auto take = [&](size_t bytes) { char* q = p; p += align16(bytes); return q; };
+    double* target = reinterpret_cast<double*>(take(nshots * 8));
+    uint32_t* blk = reinterpret_cast<uint32_t*>(take(nshots * 4));
+    uint32_t* order = reinterpret_cast<uint32_t*>(take(nshots * 4));
+    uint32_t* count = reinterpret_cast<uint32_t*>(take((size_t(nb) + 1) * 4));
+    uint32_t* cursor = reinterpret_cast<uint32_t*>(take((size_t(nb) + 1) * 4));
+    uint32_t* offset = reinterpret_cast<uint32_t*>(take((size_t(nb) + 2) * 4));
+    uint32_t* nonempty = reinterpret_cast<uint32_t*>(take(size_t(nb) * 4 + 4));
+    uint32_t* nne = reinterpret_cast<uint32_t*>(take(4));
+    // count and cursor are adjacent: one clear
+    QSE_CUDA(cudaMemsetAsync(count, 0, reinterpret_cast<char*>(offset) - reinterpret_cast<char*>(count), ctx->stream));
+    k_shot_block<<<grid, 256, 0, ctx->stream>>>(v.cin, nb, d_u, nshots, seed, st->size(), target, blk, count, d_out);
+    k_shot_offsets<<<1, kOT, 0, ctx->stream>>>(count, nb, offset, nonempty, nne);
+    k_shot_scatter<<<grid, 256, 0, ctx->stream>>>(blk, nshots, nb, offset, cursor, order);
+    // the attribute belongs to the current device: set on every call
+    QSE_CUDA(cudaFuncSetAttribute(k_block_search, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSearchSmem)));
+    const unsigned pgrid = unsigned(std::min<uint64_t>(std::min<uint64_t>(nb, nshots), uint64_t(ctx->num_sms) * kWriteCTAs));
+    k_block_search<<<pgrid, kBT, kSearchSmem, ctx->stream>>>(v.cin, v.cdf, nonempty, nne, offset, order, target, d_out);
+    QSE_CUDA(cudaGetLastError());
+    count_launch(ctx, 4);
+}
+}  // namespace
+
 void sample(qse_state* st, const double* u_host, size_t nshots, uint64_t seed, uint64_t* out_host)
 {
     qse_ctx* ctx = st->ctx;
     if (nshots == 0) return;
     CdfView v = build_cdf(st);
-    // scratch: u [nshots] | out [nshots]
-    size_t ubytes = u_host ? nshots * 8 : 0;
-    ctx->scratch.reserve(ubytes + nshots * 8 + 16);
-    double* d_u = u_host ? static_cast<double*>(ctx->scratch.ptr) : nullptr;
-    uint64_t* d_out = reinterpret_cast<uint64_t*>(static_cast<char*>(ctx->scratch.ptr) + ubytes);
-    if (u_host) QSE_CUDA(cudaMemcpyAsync(d_u, u_host, ubytes, cudaMemcpyHostToDevice, ctx->stream));
-    unsigned grid = unsigned(std::min<uint64_t>((nshots + 255) / 256, uint64_t(ctx->num_sms) * 8));
-    k_sample<<<grid, 256, 0, ctx->stream>>>(v.cdf, st->size(), v.cin, v.nb, v.bs, d_u, nshots, seed, d_out,
-                                            make_perm(st));
-    QSE_CUDA(cudaGetLastError());
-    count_launch(ctx);
+    // scratch: u [nshots] | out [nshots] | the bucketing tables
+    const size_t ubytes = u_host ? align16(nshots * 8) : 0;
+    const size_t obytes = align16(nshots * 8);
+    ctx->scratch.reserve(ubytes + obytes + sample_scratch_bytes(v.nb, nshots));
+    char* base = static_cast<char*>(ctx->scratch.ptr);
+    double* d_u = u_host ? reinterpret_cast<double*>(base) : nullptr;
+    uint64_t* d_out = reinterpret_cast<uint64_t*>(base + ubytes);
+    if (u_host) QSE_CUDA(cudaMemcpyAsync(d_u, u_host, nshots * 8, cudaMemcpyHostToDevice, ctx->stream));
+    sample_on(st, v, d_u, nshots, seed, d_out, base + ubytes + obytes);
     QSE_CUDA(cudaMemcpyAsync(out_host, d_out, nshots * 8, cudaMemcpyDeviceToHost, ctx->stream));
     QSE_CUDA(cudaStreamSynchronize(ctx->stream));
 }
@@ -1146,11 +1299,8 @@ void sample_device(qse_state* st, const double* d_u, size_t nshots, uint64_t see
     qse_ctx* ctx = st->ctx;
     if (nshots == 0) return;
     CdfView v = build_cdf(st);
-    unsigned grid = unsigned(std::min<uint64_t>((nshots + 255) / 256, uint64_t(ctx->num_sms) * 8));
-    k_sample<<<grid, 256, 0, ctx->stream>>>(v.cdf, st->size(), v.cin, v.nb, v.bs, d_u, nshots, seed, d_out,
-                                            make_perm(st));
-    QSE_CUDA(cudaGetLastError());
-    count_launch(ctx);
+    ctx->scratch.reserve(sample_scratch_bytes(v.nb, nshots));
+    sample_on(st, v, d_u, nshots, seed, d_out, static_cast<char*>(ctx->scratch.ptr));
 }
 
 uint64_t measure(qse_state* st, double u)

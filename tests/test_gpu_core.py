@@ -287,6 +287,25 @@ def test_sample_after_execute(dev, n):
         t = u[i] * cum[-1]
         assert np.min(np.abs(cum - t)) < 1e-12
 
+def test_sample_bucketed_shot_patterns(dev):
+    """The shots are bucketed by block and each block with shots rebuilds its
+    exact cumulative values in shared memory: one shot, a handful, tens of
+    thousands in one block (identical draws), draws at 0 and just below 1, and
+    every block touched -- against the oracle's sampler on the same state."""
+    n = 21
+    ops = W.random_circuit(n, 10 * n, 777)
+    st = StateVector(n, dev)
+    L.check(L.lib.qse_execute(st.handle, L.dptr(ops), len(ops), None, 0, None, None, 0, None))
+    amp = st.download()
+    cases = [np.array([0.5]), np.array([0.0, 0.999999, 0.25, 0.75, 0.5]),
+             np.full(40000, 0.3141592653589793), np.array([0.0, 1.0 - 2.0 ** -53]),
+             np.random.default_rng(21).random(300000)]
+    for u in cases:
+        out = np.empty(len(u), dtype=np.uint64)
+        L.check(L.lib.qse_sample(st.handle, u.ctypes.data_as(L._pd), len(u), 0, out.ctypes.data_as(L._pu64)))
+        assert np.array_equal(out, O.sample(amp, n, u)), len(u)
+
+
 def test_sample_exact_cdf_many_binades(dev):
     # amplitudes spread over many binades so the running sum crosses many
     # binade boundaries inside blocks (the exact scan's slow path)
@@ -492,3 +511,28 @@ def test_execute_mid_circuit_measure_and_reset(dev):
     with pytest.raises(L.QseError):
         L.check(L.lib.qse_execute_mid(st.handle, L.dptr(ops), len(ops), None, 0, u.ctypes.data_as(L._pd), 3,
                                       res.ctypes.data_as(C.POINTER(C.c_int32)), 1))
+
+
+@pytest.mark.parametrize("n", [22, 24])
+def test_streamed_passes_match_oracle(dev, n):
+    """Pass-kernel mode 2: forward read+write passes over at least 2^10 tiles
+    run as the persistent streamed kernel (bulk async copies into a three-slot
+    shared-memory ring, two compute groups).  Random circuits over every gate
+    and the H + RZ + QFT circuit against the oracle, and the same circuits
+    through the one-CTA-per-tile kernels: identical amplitudes."""
+    L.check(L.lib.qse_ctx_set_jit(dev.handle, 2))
+    try:
+        for ops in (W.random_circuit(n, 12 * n, 7000 + n), W.hrz_qft(n, seed=2)):
+            got, stats = run_gpu(dev, n, ops, fusion=True, k=12)
+            assert np.max(np.abs(got - O.run(n, ops))) <= TOL
+            L.check(L.lib.qse_ctx_set_jit(dev.handle, 1))
+            classic, _ = run_gpu(dev, n, ops, fusion=True, k=12)
+            L.check(L.lib.qse_ctx_set_jit(dev.handle, 2))
+            assert np.array_equal(got, classic)
+            # the state is the input of the next pass: an execute on top of it
+            st = StateVector(n, dev)
+            L.check(L.lib.qse_execute(st.handle, L.dptr(ops), len(ops), None, 0, None, None, 0, None))
+            L.check(L.lib.qse_execute(st.handle, L.dptr(ops), len(ops), None, 0, None, None, 0, None))
+            assert np.max(np.abs(st.download() - O.run(n, np.concatenate([ops, ops])))) <= TOL
+    finally:
+        L.check(L.lib.qse_ctx_set_jit(dev.handle, 1))

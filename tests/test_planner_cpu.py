@@ -146,3 +146,17 @@ def test_generated_pass_kernels_compile(name):
         pytest.skip("NVRTC not available: " + L.lib.qse_last_error().decode())
     L.check(rc)
     assert size.value > 0
+
+
+@pytest.mark.parametrize("n,seed", [(26, 2), (30, 2)])
+def test_streamed_pass_kernels_compile(n, seed):
+    """The persistent streamed pass kernels (qse_plan_compile with nstates = 3:
+    forward passes, streamed where a pass allows it) of the 26- and 30-qubit
+    H + RZ + QFT circuits generate and compile for sm_100a."""
+    ops = W.hrz_qft(n, seed=seed)
+    size = C.c_size_t()
+    rc = L.lib.qse_plan_compile(n, L.dptr(ops), len(ops), None, 0, 0, 3, C.byref(size))
+    if rc == 6:
+        pytest.skip("NVRTC not available: " + L.lib.qse_last_error().decode())
+    L.check(rc)
+    assert size.value > 0
