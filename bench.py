@@ -84,6 +84,9 @@ def parse():
     ap.add_argument("--no-gates", action="store_true", help="skip the per-gate drop-in comparison")
     ap.add_argument("--no-adjoint30", action="store_true", help="skip the 30-qubit adjoint section")
     ap.add_argument("--tile", type=int, default=0, help="tile qubits of the fused passes (0 = library default)")
+    ap.add_argument("--pass-kernel", type=int, default=-1, choices=[-1, 0, 1, 2],
+                    help="pass kernels (qse_ctx_set_jit): 0 interpreter, 1 one CTA per tile, 2 streamed; "
+                         "-1 = library default")
     ap.add_argument("--playground", default=None,
                     help="comma-separated playground workloads (or 'all'): the paper's construct -> execute -> "
                          "sample wall-clock timings, one JSON line instead of the step")
@@ -471,6 +474,8 @@ def main():
     dev = Device(local)
     if args.tile:
         dev.set_fusion(True, args.tile, 0)
+    if args.pass_kernel >= 0:
+        L.check(L.lib.qse_ctx_set_jit(dev.handle, args.pass_kernel))
     lib = L.lib
     st = StateVector(n, dev)
     # device buffer for the sample outcomes (value arm: results stay in HBM)
