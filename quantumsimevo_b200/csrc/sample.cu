@@ -943,41 +943,91 @@ __global__ void k_shot_block(const double* __restrict__ cin, uint32_t nb, const 
     }
 }
 
-// one CTA: offset[b] = shots in blocks < b (offset[nb] = all), and the list of
-// blocks holding at least one shot
+// offset[b] = shots in blocks < b (offset[nb] = all) and the list of blocks
+// holding at least one shot, by a three-kernel scan over chunks of kOT blocks:
+// chunk sums, an exclusive scan of the chunk sums (one CTA), then each chunk's
+// own exclusive scan plus its base
 constexpr int kOT = 1024;
-__global__ void __launch_bounds__(kOT) k_shot_offsets(const uint32_t* __restrict__ count, uint32_t nb,
-                                                      uint32_t* __restrict__ offset, uint32_t* __restrict__ nonempty,
-                                                      uint32_t* __restrict__ nne)
+
+// exclusive block-wide scan of two counters (kOT threads)
+__device__ __forceinline__ void block_scan2(uint32_t a, uint32_t b, uint32_t& ea, uint32_t& eb, uint32_t& ta,
+                                            uint32_t& tb)
 {
-    __shared__ uint32_t sa[kOT], sb[kOT];
-    const uint32_t t = threadIdx.x;
-    const uint32_t ch = (nb + kOT - 1) / kOT;
-    const uint32_t lo = min(nb, t * ch), hi = min(nb, lo + ch);
-    uint32_t a = 0, b = 0;
-    for (uint32_t i = lo; i < hi; ++i) {
-        a += count[i];
-        b += count[i] != 0u;
+    __shared__ uint32_t wa[kOT / 32], wb[kOT / 32];
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    uint32_t ia = a, ib = b;   // inclusive within the warp
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t xa = __shfl_up_sync(0xffffffffu, ia, o), xb = __shfl_up_sync(0xffffffffu, ib, o);
+        if (lane >= uint32_t(o)) { ia += xa; ib += xb; }
     }
-    sa[t] = a;
-    sb[t] = b;
+    if (lane == 31u) { wa[w] = ia; wb[w] = ib; }
     __syncthreads();
-    for (uint32_t d = 1; d < kOT; d <<= 1) {   // inclusive scan (Hillis-Steele)
-        const uint32_t xa = t >= d ? sa[t - d] : 0u, xb = t >= d ? sb[t - d] : 0u;
-        __syncthreads();
-        sa[t] += xa;
-        sb[t] += xb;
-        __syncthreads();
+    if (w == 0) {
+        uint32_t va = wa[lane], vb = wb[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t xa = __shfl_up_sync(0xffffffffu, va, o), xb = __shfl_up_sync(0xffffffffu, vb, o);
+            if (lane >= uint32_t(o)) { va += xa; vb += xb; }
+        }
+        wa[lane] = va;   // inclusive over warps
+        wb[lane] = vb;
     }
-    uint32_t ea = sa[t] - a, eb = sb[t] - b;
-    for (uint32_t i = lo; i < hi; ++i) {
-        offset[i] = ea;
-        ea += count[i];
-        if (count[i]) nonempty[eb++] = i;
+    __syncthreads();
+    const uint32_t ba = w ? wa[w - 1] : 0u, bb = w ? wb[w - 1] : 0u;
+    ea = ba + ia - a;
+    eb = bb + ib - b;
+    ta = wa[kOT / 32 - 1];
+    tb = wb[kOT / 32 - 1];
+    __syncthreads();   // wa / wb are reused by the next call
+}
+
+__global__ void __launch_bounds__(kOT) k_scan_part(const uint32_t* __restrict__ count, uint32_t nb,
+                                                   uint32_t* __restrict__ psum, uint32_t* __restrict__ pnz)
+{
+    const uint32_t i = blockIdx.x * kOT + threadIdx.x;
+    const uint32_t c = i < nb ? count[i] : 0u;
+    uint32_t ea, eb, ta, tb;
+    block_scan2(c, c != 0u, ea, eb, ta, tb);
+    if (threadIdx.x == 0) {
+        psum[blockIdx.x] = ta;
+        pnz[blockIdx.x] = tb;
     }
-    if (t == kOT - 1) {
-        offset[nb] = sa[t];
-        *nne = sb[t];
+}
+
+// one CTA: the chunk sums become exclusive prefixes (in place); totals to offset[nb] and *nne
+__global__ void __launch_bounds__(kOT) k_scan_top(uint32_t* __restrict__ psum, uint32_t* __restrict__ pnz,
+                                                  uint32_t nchunks, uint32_t* __restrict__ offset_end,
+                                                  uint32_t* __restrict__ nne)
+{
+    uint32_t carry_a = 0, carry_b = 0;
+    for (uint32_t base = 0; base < nchunks; base += kOT) {
+        const uint32_t i = base + threadIdx.x;
+        const uint32_t a = i < nchunks ? psum[i] : 0u, b = i < nchunks ? pnz[i] : 0u;
+        uint32_t ea, eb, ta, tb;
+        block_scan2(a, b, ea, eb, ta, tb);
+        if (i < nchunks) {
+            psum[i] = carry_a + ea;
+            pnz[i] = carry_b + eb;
+        }
+        carry_a += ta;
+        carry_b += tb;
+    }
+    if (threadIdx.x == 0) {
+        *offset_end = carry_a;
+        *nne = carry_b;
+    }
+}
+
+__global__ void __launch_bounds__(kOT) k_scan_final(const uint32_t* __restrict__ count, uint32_t nb,
+                                                    const uint32_t* __restrict__ psum, const uint32_t* __restrict__ pnz,
+                                                    uint32_t* __restrict__ offset, uint32_t* __restrict__ nonempty)
+{
+    const uint32_t i = blockIdx.x * kOT + threadIdx.x;
+    const uint32_t c = i < nb ? count[i] : 0u;
+    uint32_t ea, eb, ta, tb;
+    block_scan2(c, c != 0u, ea, eb, ta, tb);
+    if (i < nb) {
+        offset[i] = psum[blockIdx.x] + ea;
+        if (c) nonempty[pnz[blockIdx.x] + eb] = i;
     }
 }
 
@@ -991,6 +1041,52 @@ __global__ void k_shot_scatter(const uint32_t* __restrict__ blk, uint64_t nshots
         if (b < nb) order[offset[b] + atomicAdd(cursor + b, 1u)] = uint32_t(s);
     }
 }
+
+// A few shots (a measure(), a short sample): one CTA per shot finds the shot's
+// block, rebuilds that block's exact cumulative values in shared memory and
+// answers the shot -- no bucketing pass over every block.
+__global__ void __launch_bounds__(kBT) k_search_each(const double* __restrict__ cin, const double* __restrict__ prob,
+                                                     uint32_t nb, const double* __restrict__ u, uint64_t seed,
+                                                     uint64_t size, uint64_t* __restrict__ out)
+{
+    __shared__ uint64_t sh[160];
+    __shared__ double s_t;
+    __shared__ uint32_t s_b;
+    extern __shared__ double stg[];
+    double* const cum = stg + kBT * kPad;
+    const uint64_t s = blockIdx.x;
+    if (threadIdx.x == 0) {
+        double us;
+        if (u) us = u[s];
+        else {
+            double u2;
+            philox_uniform_pair(seed, s, kTagSample, us, u2);
+        }
+        const double t = __dadd_rn(__dmul_rn(us, cin[nb]), 0.0);
+        uint64_t lo = 0, len = nb;
+        while (len > 0) {
+            uint64_t half = len >> 1, mid = lo + half;
+            if (cin[mid + 1] < t) { lo = mid + 1; len = len - half - 1; }
+            else len = half;
+        }
+        s_t = t;
+        s_b = uint32_t(lo);
+    }
+    __syncthreads();
+    const uint32_t b = s_b;
+    if (b >= nb) {
+        if (threadIdx.x == 0) out[s] = size;   // beyond the end: lower_bound returns size
+        return;
+    }
+    stage_async(stg, prob, uint64_t(b) * kBS);
+    stage_wait<0>();
+    __syncthreads();
+    block_exact(kBS, cin[b], cum, sh, stg);
+    __syncthreads();
+    if (threadIdx.x == 0) out[s] = uint64_t(b) * kBS + lower_bound_dev(cum, kBS, s_t);
+}
+constexpr size_t kEachSmem = (size_t(kBT) * kPad + kBS) * sizeof(double);
+constexpr size_t kFewShots = 64;
 
 // shared memory of k_block_search: two staging buffers + one block's cumulative values
 constexpr size_t kSearchSmem = kStage2 + size_t(kBS) * sizeof(double);
@@ -1235,8 +1331,9 @@ size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 // into d_out.  `scratch` must hold sample_scratch_bytes(nb, nshots) bytes.
 size_t sample_scratch_bytes(uint32_t nb, size_t nshots)
 {
+    const size_t nchunks = (size_t(nb) + kOT - 1) / kOT;
     return align16(nshots * 8) + 2 * align16(nshots * 4) + 2 * align16((size_t(nb) + 1) * 4) +
-           align16((size_t(nb) + 2) * 4) + align16(size_t(nb) * 4 + 4) + 16;
+           align16((size_t(nb) + 2) * 4) + align16(size_t(nb) * 4 + 4) + align16(4) + 2 * align16(nchunks * 4) + 16;
 }
 
 void sample_on(qse_state* st, const CdfView& v, const double* d_u, size_t nshots, uint64_t seed, uint64_t* d_out,
@@ -1252,6 +1349,14 @@ void sample_on(qse_state* st, const CdfView& v, const double* d_u, size_t nshots
         return;
     }
     const uint32_t nb = v.nb;
+    if (nshots <= kFewShots) {
+        QSE_CUDA(cudaFuncSetAttribute(k_search_each, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kEachSmem)));
+        k_search_each<<<unsigned(nshots), kBT, kEachSmem, ctx->stream>>>(v.cin, v.cdf, nb, d_u, seed, st->size(), d_out);
+        QSE_CUDA(cudaGetLastError());
+        count_launch(ctx);
+        return;
+    }
+    const uint32_t nchunks = (nb + kOT - 1) / kOT;
     char* p = scratch;
     auto take = [&](size_t bytes) { char* q = p; p += align16(bytes); return q; };
     double* target = reinterpret_cast<double*>(take(nshots * 8));
@@ -1262,17 +1367,21 @@ void sample_on(qse_state* st, const CdfView& v, const double* d_u, size_t nshots
     uint32_t* offset = reinterpret_cast<uint32_t*>(take((size_t(nb) + 2) * 4));
     uint32_t* nonempty = reinterpret_cast<uint32_t*>(take(size_t(nb) * 4 + 4));
     uint32_t* nne = reinterpret_cast<uint32_t*>(take(4));
+    uint32_t* psum = reinterpret_cast<uint32_t*>(take(size_t(nchunks) * 4));
+    uint32_t* pnz = reinterpret_cast<uint32_t*>(take(size_t(nchunks) * 4));
     // count and cursor are adjacent: one clear
     QSE_CUDA(cudaMemsetAsync(count, 0, reinterpret_cast<char*>(offset) - reinterpret_cast<char*>(count), ctx->stream));
     k_shot_block<<<grid, 256, 0, ctx->stream>>>(v.cin, nb, d_u, nshots, seed, st->size(), target, blk, count, d_out);
-    k_shot_offsets<<<1, kOT, 0, ctx->stream>>>(count, nb, offset, nonempty, nne);
+    k_scan_part<<<nchunks, kOT, 0, ctx->stream>>>(count, nb, psum, pnz);
+    k_scan_top<<<1, kOT, 0, ctx->stream>>>(psum, pnz, nchunks, offset + nb, nne);
+    k_scan_final<<<nchunks, kOT, 0, ctx->stream>>>(count, nb, psum, pnz, offset, nonempty);
     k_shot_scatter<<<grid, 256, 0, ctx->stream>>>(blk, nshots, nb, offset, cursor, order);
     // the attribute belongs to the current device: set on every call
     QSE_CUDA(cudaFuncSetAttribute(k_block_search, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kSearchSmem)));
     const unsigned pgrid = unsigned(std::min<uint64_t>(std::min<uint64_t>(nb, nshots), uint64_t(ctx->num_sms) * kWriteCTAs));
     k_block_search<<<pgrid, kBT, kSearchSmem, ctx->stream>>>(v.cin, v.cdf, nonempty, nne, offset, order, target, d_out);
     QSE_CUDA(cudaGetLastError());
-    count_launch(ctx, 4);
+    count_launch(ctx, 6);
 }
 }  // namespace
 
