@@ -173,6 +173,7 @@ int qse_ctx_destroy(qse_ctx* ctx)
     ctx->plan_buf.release();
     ctx->scratch.release();
     ctx->scratch2.release();
+    ctx->gv_buf.release();
     ctx->plan_host.release();
     ctx->host_small.release();
     ctx->host_small2.release();
@@ -611,7 +612,7 @@ int qse_plan_compile(uint32_t nqubits, const qse_op* ops, size_t nops, const dou
     size_t total = 0;
     std::set<std::string> done;   // identical passes share one kernel, as in execution
     for (const auto& p : pl.passes) {
-        qse::jit::Source s = qse::jit::generate(p, nstates, false, streamed);
+        qse::jit::Source s = qse::jit::generate(p, nstates, false, streamed, nqubits >= qse::jit::kPreGroupQubits);
         total += s.code.size();
         if (done.insert(s.code).second) qse::jit::compile_only(s);
     }

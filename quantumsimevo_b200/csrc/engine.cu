@@ -100,8 +100,9 @@ void apply_plain(qse_state* st, const plan::Gate& g)
         return;
     }
     case QSE_GATE_SWAP:
-        if (g.t == g.c) return;
-        launch_swap(st, P[g.t], P[g.c]);
+        // a relabelling of the logical -> physical map: no amplitude moves
+        // (downloads, samples and later gates read through the map)
+        if (g.t != g.c) std::swap(st->perm[g.t], st->perm[g.c]);
         return;
     case QSE_GATE_2X2: launch_gate2x2(st, P[g.t], g.m, 0); return;
     default: fail(QSE_ERR_UNSUPPORTED, "gate type not executable");
@@ -164,6 +165,38 @@ Uploaded upload_plan(qse_ctx* ctx, const plan::Plan& pl)
     return up;
 }
 
+// The per-CTA values of a pass's diagonal groups, one row of ng values per tile:
+// group g of tile t sums the angles of its terms whose outer-qubit conditions
+// hold for t's outer bits (t's bits deposited on the outer positions in
+// ascending order, as the pass kernel numbers its CTAs), then (cos, sin) for
+// direct groups.  Same sums, in the same order, as the prologue a pass kernel
+// otherwise runs per CTA; here they run on the whole GPU ahead of the pass, so
+// the pass starts its arithmetic without a per-CTA sincos chain and barriers.
+__global__ void __launch_bounds__(256) k_group_values(const plan::TermRec* __restrict__ terms,
+                                                      const plan::GroupRec* __restrict__ groups, uint32_t ng,
+                                                      uint64_t outer_mask, uint64_t ntiles, double2* __restrict__ out)
+{
+    const uint64_t total = ntiles * ng;
+    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < total; i += uint64_t(gridDim.x) * blockDim.x) {
+        const uint64_t tile = i / ng;
+        const uint32_t g = uint32_t(i - tile * ng);
+        uint64_t ob = 0, c = tile;
+        for (uint64_t m = outer_mask; m; m &= m - 1) {
+            ob |= (c & 1ull) << (__ffsll((long long)m) - 1);
+            c >>= 1;
+        }
+        const plan::GroupRec gr = groups[g];
+        double th = 0.0;
+        for (uint32_t k = 0; k < gr.count; ++k) {
+            const plan::TermRec t = terms[gr.first + k];
+            if ((ob & t.ocond) == t.ocond) th += t.theta;
+        }
+        double s, co;
+        if (gr.direct) sincos(th, &s, &co);
+        out[i] = gr.direct ? make_double2(co, s) : make_double2(th, 0.0);
+    }
+}
+
 // Specialised pass kernels repay their compile time (NVRTC: about a second or
 // more per distinct kernel) when a pass is expensive, i.e. on large states, or
 // when few of a plan's kernels are new.  A deep circuit on a small state can
@@ -184,7 +217,8 @@ plan::Plan plan_for(qse_state* st, const std::vector<plan::Gate>& gates, plan::O
     if (!use_jit) return pl;
     srcs.reserve(pl.passes.size());
     for (size_t i = 0; i < pl.passes.size(); ++i)
-        srcs.push_back(jit::generate(pl.passes[i], ns, i == 0 && ns == 1 && st->lazy_basis, st->ctx->jit == 2));
+        srcs.push_back(jit::generate(pl.passes[i], ns, i == 0 && ns == 1 && st->lazy_basis, st->ctx->jit == 2,
+                                     st->n >= jit::kPreGroupQubits));
     if (st->n >= kJitAlwaysQubits || jit::count_uncached(srcs) <= kJitMaxNewKernels) return pl;
     use_jit = false;
     srcs.clear();
@@ -233,8 +267,20 @@ struct PassRunner {
             nvtxRangePop();
             return;
         }
+        const void* gvt = nullptr;
+        if (srcs[i].pre_gv) {
+            const uint64_t ntiles = uint64_t(1) << (st->n - kq[i]);
+            const uint64_t cnt = ntiles * srcs[i].ngroups;
+            ctx->gv_buf.reserve(cnt * sizeof(double2));
+            const uint64_t blocks = std::min<uint64_t>((cnt + 255) / 256, uint64_t(ctx->num_sms) * 32);
+            k_group_values<<<unsigned(blocks), 256, 0, ctx->stream>>>(a.terms, a.groups, srcs[i].ngroups, a.outer_mask,
+                                                                      ntiles, static_cast<double2*>(ctx->gv_buf.ptr));
+            QSE_CUDA(cudaGetLastError());
+            count_launch(ctx);
+            gvt = ctx->gv_buf.ptr;
+        }
         cudaEvent_t stop = tile::pass_timer_begin(ctx);
-        jit::launch(ctx, *ks[i], srcs[i], st->n, kq[i], a.psi, lam, a.terms, a.groups, part, st->lazy_index);
+        jit::launch(ctx, *ks[i], srcs[i], st->n, kq[i], a.psi, lam, a.terms, a.groups, part, st->lazy_index, gvt);
         tile::pass_timer_end(ctx, stop);
         count_launch(ctx);
         nvtxRangePop();

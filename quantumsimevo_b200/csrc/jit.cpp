@@ -98,9 +98,15 @@ struct Gen {
     int basis_slot = -1;    // prm slot of bi (set per launch)
     bool xb_used = false;   // the exchange buffer holds data some thread may still read
     std::string SYNC = "__syncthreads();";   // barrier of the threads that share xb
+    // the per-CTA group values come precomputed from global memory (gvt, one row
+    // of ng values per tile): no prologue, no lane tables, no barrier before the body
+    bool pre_gv = false;
 
-    Gen(const plan::PassProgram& p, int nstates, bool zero_input) : P(p), ns(nstates), zero_in(zero_input && nstates == 1)
+    Gen(const plan::PassProgram& p, int nstates, bool zero_input, bool precomputed_groups = false)
+        : P(p), ns(nstates), zero_in(zero_input && nstates == 1),
+          pre_gv(precomputed_groups && !(zero_input && nstates == 1) && !p.groups.empty())
     {
+        if (pre_gv) max_tables = 0;
         R = 1u << P.rb;
         T = 1u << (P.k - P.rb);
         NW = std::max(1u, T / 32);
@@ -223,6 +229,7 @@ struct Gen {
     struct Item { uint16_t tcond; uint16_t g; };
     struct Fac { std::vector<Item> items; bool hc = false; double ca = 1.0, cb = 0.0; };
     static constexpr uint32_t kMaxTables = 32;
+    uint32_t max_tables = kMaxTables;   // 0 with precomputed group values (no prologue)
     std::vector<plan::KOp> run_ops;
     std::vector<Item> chain[5];   // pending accumulator groups: ar0..ar3, at
     std::ostringstream tabs;      // prologue code building the lane tables
@@ -260,7 +267,7 @@ struct Gen {
             push(F.cb);
             cst = "make_double2(P.v[" + std::to_string(ci) + "], P.v[" + std::to_string(ci + 1) + "])";
         }
-        if (ntab < kMaxTables && (L.size() >= 2 || (L.size() == 1 && F.hc))) {
+        if (ntab < max_tables && (L.size() >= 2 || (L.size() == 1 && F.hc))) {
             const uint32_t t = ntab++;
             tabs << "  if ((tid >> 5) == " << (t % NW) << "u) { const u32 l = tid & 31u; double2 v = "
                  << (F.hc ? cst : std::string("make_double2(1.0, 0.0)")) << ";";
@@ -411,9 +418,14 @@ struct Gen {
         o << "  const u32 tid = threadIdx.x;\n";
         o << "  extern __shared__ double2 sm[];\n";
         o << "  double2* xb = sm; (void)xb;\n";
-        o << "  double2* gv = sm + " << tsize << "; (void)gv;\n";
-        o << "  double2* tb = gv + " << ng << "; (void)tb;\n";
-        if (ns == 2) o << "  double* wp = reinterpret_cast<double*>(tb + " << 32 * ntab << ");\n";
+        if (pre_gv) {
+            o << "  const double2* __restrict__ gv = gvt + (u64)blockIdx.x * " << ng << "u;\n";
+            if (ns == 2) o << "  double* wp = reinterpret_cast<double*>(sm + " << tsize << ");\n";
+        } else {
+            o << "  double2* gv = sm + " << tsize << "; (void)gv;\n";
+            o << "  double2* tb = gv + " << ng << "; (void)tb;\n";
+            if (ns == 2) o << "  double* wp = reinterpret_cast<double*>(tb + " << 32 * ntab << ");\n";
+        }
         // outer base
         o << "  u64 ob = 0;\n  { u64 c = blockIdx.x;";
         for (uint32_t q = 0; q < 64; ++q)
@@ -454,7 +466,7 @@ struct Gen {
             }
         }
         // prologue: per-CTA diagonal group values, then the lane tables
-        if (ng) {
+        if (ng && !pre_gv) {
             // the pass's terms are first copied into the exchange buffer (unused until
             // the first layout exchange, which follows the prologue's barrier) by every
             // thread at once, so the per-group sums read shared memory instead of
@@ -473,7 +485,7 @@ struct Gen {
         }
         if (ntab) o << "  __syncthreads();\n" << tabs.str();
         if (ns == 2 && nslots) o << "  for (u32 i = tid; i < " << nslots * NW << "u; i += " << T << "u) wp[i] = 0.0;\n";
-        o << "  __syncthreads();\n";
+        if (!pre_gv || (ns == 2 && nslots)) o << "  __syncthreads();\n";
         if (zero_in)
             for (uint32_t j = 0; j < R; ++j)
                 o << "  a0[" << j << "] = make_double2((gb | " << hex(reg_off(j)) << ") == bi ? 1.0 : 0.0, 0.0);\n";
@@ -487,8 +499,8 @@ struct Gen {
         src << "extern \"C\" __global__ void __launch_bounds__(" << T << ", " << min_blocks << ") qse_pass("
             << "double2* __restrict__ psi, double2* __restrict__ lam, const TermRec* __restrict__ terms, "
             << "const GroupRec* __restrict__ groups, double* __restrict__ slot_partial, u32* __restrict__ status, "
-            << "const __grid_constant__ Prm P)\n{\n"
-            << "  (void)lam; (void)terms; (void)groups; (void)slot_partial; (void)status;\n"
+            << "const double2* __restrict__ gvt, const __grid_constant__ Prm P)\n{\n"
+            << "  (void)lam; (void)terms; (void)groups; (void)slot_partial; (void)status; (void)gvt;\n"
             << head.str() << ops_txt << "}\n";
         return src.str();
     }
@@ -575,8 +587,8 @@ struct Gen {
         s << "extern \"C\" __global__ void __launch_bounds__(" << nth << ", 1) qse_pass("
           << "double2* __restrict__ psi, double2* __restrict__ lam, const TermRec* __restrict__ terms, "
           << "const GroupRec* __restrict__ groups, double* __restrict__ slot_partial, u32* __restrict__ status, "
-          << "const __grid_constant__ Prm P)\n{\n"
-          << "  (void)lam; (void)slot_partial;\n"
+          << "const double2* __restrict__ gvt, const __grid_constant__ Prm P)\n{\n"
+          << "  (void)lam; (void)slot_partial; (void)gvt;\n"
           << "  extern __shared__ __align__(128) double2 sm[];\n"
           << "  u64* const bar = reinterpret_cast<u64*>(sm + " << 3 * tsize << ");   // one per slot\n"
           << "  u32* const nfill = reinterpret_cast<u32*>(bar + 4);                   // copies issued per slot\n"
@@ -810,7 +822,7 @@ static bool streamable(const plan::PassProgram& p, int nstates, bool basis_input
            __builtin_popcountll(p.outer_mask) >= 10;
 }
 
-Source generate(const plan::PassProgram& p, int nstates, bool basis_input, bool streamed)
+Source generate(const plan::PassProgram& p, int nstates, bool basis_input, bool streamed, bool precomputed_groups)
 {
     if (streamed && streamable(p, nstates, basis_input)) {
         Gen g(p, nstates, false);
@@ -824,11 +836,13 @@ Source generate(const plan::PassProgram& p, int nstates, bool basis_input, bool 
             return s;
         }
     }
-    Gen g(p, nstates, basis_input);
+    Gen g(p, nstates, basis_input, precomputed_groups);
     Source s;
     s.code = g.run();
     s.prm = std::move(g.prm);
     s.basis_slot = g.basis_slot;
+    s.pre_gv = g.pre_gv;
+    s.ngroups = uint32_t(p.groups.size());
     s.threads = g.T;
     s.smem = (size_t(1) << p.k) * 16 + p.groups.size() * 16 + size_t(g.ntab) * 32 * 16 +
              (nstates == 2 ? p.slot_src.size() * g.NW * 8 : 0);
@@ -887,7 +901,7 @@ std::vector<std::shared_ptr<Kernel>> get_kernels(const std::vector<const Source*
 }
 
 void launch(qse_ctx* ctx, Kernel& k, const Source& s, uint32_t n, uint32_t kq, void* psi, void* lam,
-            const void* terms, const void* groups, double* slot_partial, uint64_t basis_index)
+            const void* terms, const void* groups, double* slot_partial, uint64_t basis_index, const void* gvt)
 {
     unsigned* status = ctx->status_dev;
     if (s.smem > ctx->smem_optin) fail(QSE_ERR_SIZE, "pass needs more shared memory than the device offers");
@@ -900,7 +914,7 @@ void launch(qse_ctx* ctx, Kernel& k, const Source& s, uint32_t n, uint32_t kq, v
     if (s.basis_slot >= 0) prm[size_t(s.basis_slot)] = double(basis_index);   // exact below 2^53
     if (prm.empty()) prm.push_back(0.0);
     void* args[] = {&psi, &lam, const_cast<const void**>(&terms), const_cast<const void**>(&groups), &slot_partial,
-                    &status, prm.data()};
+                    &status, const_cast<const void**>(&gvt), prm.data()};
     // streamed passes: one persistent CTA per SM; otherwise one CTA per tile
     const uint64_t tiles = uint64_t(1) << (n - kq);
     const uint64_t grid = s.streamed ? std::min<uint64_t>(tiles, uint64_t(ctx->num_sms)) : tiles;

@@ -21,7 +21,14 @@ struct Source {
     size_t smem = 0;
     int basis_slot = -1;      // basis-input passes: the prm slot that takes the basis index
     bool streamed = false;    // persistent streamed kernel (grid = SM count) instead of one CTA per tile
+    bool pre_gv = false;      // the per-CTA group values are read from a precomputed table (gvt)
+    uint32_t ngroups = 0;     // diagonal groups of the pass (the table's row length)
 };
+
+// States of at least this many qubits run their passes with the group values
+// precomputed per tile (the table costs one small kernel and 16 B per group and
+// tile; on small states the in-kernel prologue is cheaper than a launch)
+constexpr uint32_t kPreGroupQubits = 22;
 
 // dynamic shared memory a streamed pass may use (227 KiB per CTA on sm_100)
 constexpr size_t kStreamedSmemMax = 227 * 1024;
@@ -42,14 +49,19 @@ size_t compile_only(const Source& s);
 // streamed: use the persistent streamed kernel when the pass allows it (forward
 // read+write passes of 12 tile qubits over at least 2^10 tiles, pieces of at
 // least 8 contiguous amplitudes); otherwise one CTA per tile
-Source generate(const plan::PassProgram& p, int nstates, bool basis_input = false, bool streamed = false);
+// precomputed_groups: the pass reads its per-CTA diagonal group values from a
+// table computed beforehand (k_group_values: one row of ngroups values per
+// tile) instead of computing them in a prologue; not for basis-input passes
+Source generate(const plan::PassProgram& p, int nstates, bool basis_input = false, bool streamed = false,
+                bool precomputed_groups = false);
 // distinct sources among srcs that are not compiled yet
 size_t count_uncached(const std::vector<Source>& srcs);
 // compiled kernels for every source (cached by source text; missing ones are compiled in parallel)
 std::vector<std::shared_ptr<Kernel>> get_kernels(const std::vector<const Source*>& srcs);
 // basis_index: the physical index of a basis-input pass's input state (ignored otherwise)
 void launch(qse_ctx* ctx, Kernel& k, const Source& s, uint32_t n, uint32_t kq, void* psi, void* lam,
-            const void* terms, const void* groups, double* slot_partial, uint64_t basis_index = 0);
+            const void* terms, const void* groups, double* slot_partial, uint64_t basis_index = 0,
+            const void* gvt = nullptr);
 
 }  // namespace jit
 }  // namespace qse

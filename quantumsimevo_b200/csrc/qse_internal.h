@@ -68,6 +68,7 @@ struct qse_ctx {
     qse::HostBuf plan_host;  // pinned staging for the pass programs
     qse::DevBuf scratch;     // reductions, sampling, noise decisions
     qse::DevBuf scratch2;
+    qse::DevBuf gv_buf;      // per-tile group values of the pass being launched (precomputed)
     qse::HostBuf host_small; // pinned small results
     qse::HostBuf host_small2;
     cudaEvent_t plan_event = nullptr;  // last H2D copy out of plan_host

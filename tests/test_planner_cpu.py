@@ -160,3 +160,24 @@ def test_streamed_pass_kernels_compile(n, seed):
         pytest.skip("NVRTC not available: " + L.lib.qse_last_error().decode())
     L.check(rc)
     assert size.value > 0
+
+
+@pytest.mark.parametrize("name", ["qft26", "qaoa24_adjoint"])
+def test_precomputed_group_kernels_compile(name):
+    """States of 22 qubits and more run their passes with the per-tile group
+    values precomputed (no prologue in the pass kernel): forward passes of the
+    26-qubit H + RZ + QFT circuit and adjoint reverse passes of 24-qubit QAOA
+    generate and compile for sm_100a in that form."""
+    if name == "qft26":
+        n, ops, params, ns = 26, W.hrz_qft(26, seed=2), None, 1
+    else:
+        ops, params, _, _ = W.qaoa_maxcut(24, 2, seed=3)
+        n, ns = 24, 2
+    size = C.c_size_t()
+    p = None if params is None else np.ascontiguousarray(params)
+    rc = L.lib.qse_plan_compile(n, L.dptr(ops), len(ops), p.ctypes.data_as(L._pd) if p is not None else None,
+                                0 if p is None else p.size, 0, ns, C.byref(size))
+    if rc == 6:
+        pytest.skip("NVRTC not available: " + L.lib.qse_last_error().decode())
+    L.check(rc)
+    assert size.value > 0
