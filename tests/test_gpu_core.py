@@ -519,7 +519,9 @@ def test_streamed_passes_match_oracle(dev, n):
     run as the persistent streamed kernel (bulk async copies into a three-slot
     shared-memory ring, two compute groups).  Random circuits over every gate
     and the H + RZ + QFT circuit against the oracle, and the same circuits
-    through the one-CTA-per-tile kernels: identical amplitudes."""
+    through the one-CTA-per-tile kernels (which on these sizes take their group
+    values from the precomputed table, so the phase products round in another
+    order): equal within the amplitude tolerance."""
     L.check(L.lib.qse_ctx_set_jit(dev.handle, 2))
     try:
         for ops in (W.random_circuit(n, 12 * n, 7000 + n), W.hrz_qft(n, seed=2)):
@@ -528,7 +530,7 @@ def test_streamed_passes_match_oracle(dev, n):
             L.check(L.lib.qse_ctx_set_jit(dev.handle, 1))
             classic, _ = run_gpu(dev, n, ops, fusion=True, k=12)
             L.check(L.lib.qse_ctx_set_jit(dev.handle, 2))
-            assert np.array_equal(got, classic)
+            assert np.max(np.abs(got - classic)) <= TOL
             # the state is the input of the next pass: an execute on top of it
             st = StateVector(n, dev)
             L.check(L.lib.qse_execute(st.handle, L.dptr(ops), len(ops), None, 0, None, None, 0, None))
