@@ -99,14 +99,14 @@ struct Gen {
     bool xb_used = false;   // the exchange buffer holds data some thread may still read
     std::string SYNC = "__syncthreads();";   // barrier of the threads that share xb
     // the per-CTA group values come precomputed from global memory (gvt, one row
-    // of ng values per tile): no prologue, no lane tables, no barrier before the body
+    // of ng values per tile): the prologue copies them instead of summing terms
+    // and calling sincos per group
     bool pre_gv = false;
 
     Gen(const plan::PassProgram& p, int nstates, bool zero_input, bool precomputed_groups = false)
         : P(p), ns(nstates), zero_in(zero_input && nstates == 1),
           pre_gv(precomputed_groups && !(zero_input && nstates == 1) && !p.groups.empty())
     {
-        if (pre_gv) max_tables = 0;
         R = 1u << P.rb;
         T = 1u << (P.k - P.rb);
         NW = std::max(1u, T / 32);
@@ -418,14 +418,9 @@ struct Gen {
         o << "  const u32 tid = threadIdx.x;\n";
         o << "  extern __shared__ double2 sm[];\n";
         o << "  double2* xb = sm; (void)xb;\n";
-        if (pre_gv) {
-            o << "  const double2* __restrict__ gv = gvt + (u64)blockIdx.x * " << ng << "u;\n";
-            if (ns == 2) o << "  double* wp = reinterpret_cast<double*>(sm + " << tsize << ");\n";
-        } else {
-            o << "  double2* gv = sm + " << tsize << "; (void)gv;\n";
-            o << "  double2* tb = gv + " << ng << "; (void)tb;\n";
-            if (ns == 2) o << "  double* wp = reinterpret_cast<double*>(tb + " << 32 * ntab << ");\n";
-        }
+        o << "  double2* gv = sm + " << tsize << "; (void)gv;\n";
+        o << "  double2* tb = gv + " << ng << "; (void)tb;\n";
+        if (ns == 2) o << "  double* wp = reinterpret_cast<double*>(tb + " << 32 * ntab << ");\n";
         // outer base
         o << "  u64 ob = 0;\n  { u64 c = blockIdx.x;";
         for (uint32_t q = 0; q < 64; ++q)
@@ -466,7 +461,10 @@ struct Gen {
             }
         }
         // prologue: per-CTA diagonal group values, then the lane tables
-        if (ng && !pre_gv) {
+        if (ng && pre_gv) {
+            o << "  for (u32 g = tid; g < " << ng << "u; g += " << T << "u) gv[g] = gvt[(u64)blockIdx.x * " << ng
+              << "u + g];\n";
+        } else if (ng) {
             // the pass's terms are first copied into the exchange buffer (unused until
             // the first layout exchange, which follows the prologue's barrier) by every
             // thread at once, so the per-group sums read shared memory instead of
@@ -485,7 +483,7 @@ struct Gen {
         }
         if (ntab) o << "  __syncthreads();\n" << tabs.str();
         if (ns == 2 && nslots) o << "  for (u32 i = tid; i < " << nslots * NW << "u; i += " << T << "u) wp[i] = 0.0;\n";
-        if (!pre_gv || (ns == 2 && nslots)) o << "  __syncthreads();\n";
+        o << "  __syncthreads();\n";
         if (zero_in)
             for (uint32_t j = 0; j < R; ++j)
                 o << "  a0[" << j << "] = make_double2((gb | " << hex(reg_off(j)) << ") == bi ? 1.0 : 0.0, 0.0);\n";
