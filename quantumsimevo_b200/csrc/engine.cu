@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <map>
 
 #include "jit.h"
 #include "planner.h"
@@ -165,27 +166,27 @@ Uploaded upload_plan(qse_ctx* ctx, const plan::Plan& pl)
     return up;
 }
 
-// The per-CTA values of a pass's diagonal groups, one row of ng values per tile:
-// group g of tile t sums the angles of its terms whose outer-qubit conditions
-// hold for t's outer bits (t's bits deposited on the outer positions in
-// ascending order, as the pass kernel numbers its CTAs), then (cos, sin) for
+// The per-CTA values of a pass's diagonal groups, group-major (out[g * ntiles +
+// t]): group g of tile t sums the angles of its terms whose outer-qubit
+// conditions hold for t's outer bits (t's bits deposited on the outer positions
+// in ascending order, as the pass kernel numbers its CTAs), then (cos, sin) for
 // direct groups.  Same sums, in the same order, as the prologue a pass kernel
 // otherwise runs per CTA; here they run on the whole GPU ahead of the pass, so
-// the pass starts its arithmetic without a per-CTA sincos chain and barriers.
+// the pass starts its arithmetic without a per-CTA sincos chain.  Grid: tiles
+// along x, groups along y (a group's terms are read by the whole warp at once).
 __global__ void __launch_bounds__(256) k_group_values(const plan::TermRec* __restrict__ terms,
-                                                      const plan::GroupRec* __restrict__ groups, uint32_t ng,
-                                                      uint64_t outer_mask, uint64_t ntiles, double2* __restrict__ out)
+                                                      const plan::GroupRec* __restrict__ groups, uint64_t outer_mask,
+                                                      uint64_t ntiles, double2* __restrict__ out)
 {
-    const uint64_t total = ntiles * ng;
-    for (uint64_t i = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; i < total; i += uint64_t(gridDim.x) * blockDim.x) {
-        const uint64_t tile = i / ng;
-        const uint32_t g = uint32_t(i - tile * ng);
+    const uint32_t g = blockIdx.y;
+    const plan::GroupRec gr = groups[g];
+    for (uint64_t tile = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; tile < ntiles;
+         tile += uint64_t(gridDim.x) * blockDim.x) {
         uint64_t ob = 0, c = tile;
         for (uint64_t m = outer_mask; m; m &= m - 1) {
             ob |= (c & 1ull) << (__ffsll((long long)m) - 1);
             c >>= 1;
         }
-        const plan::GroupRec gr = groups[g];
         double th = 0.0;
         for (uint32_t k = 0; k < gr.count; ++k) {
             const plan::TermRec t = terms[gr.first + k];
@@ -193,7 +194,7 @@ __global__ void __launch_bounds__(256) k_group_values(const plan::TermRec* __res
         }
         double s, co;
         if (gr.direct) sincos(th, &s, &co);
-        out[i] = gr.direct ? make_double2(co, s) : make_double2(th, 0.0);
+        out[uint64_t(g) * ntiles + tile] = gr.direct ? make_double2(co, s) : make_double2(th, 0.0);
     }
 }
 
@@ -272,9 +273,9 @@ struct PassRunner {
             const uint64_t ntiles = uint64_t(1) << (st->n - kq[i]);
             const uint64_t cnt = ntiles * srcs[i].ngroups;
             ctx->gv_buf.reserve(cnt * sizeof(double2));
-            const uint64_t blocks = std::min<uint64_t>((cnt + 255) / 256, uint64_t(ctx->num_sms) * 32);
-            k_group_values<<<unsigned(blocks), 256, 0, ctx->stream>>>(a.terms, a.groups, srcs[i].ngroups, a.outer_mask,
-                                                                      ntiles, static_cast<double2*>(ctx->gv_buf.ptr));
+            const dim3 grid(unsigned(std::min<uint64_t>((ntiles + 255) / 256, 65535)), srcs[i].ngroups);
+            k_group_values<<<grid, 256, 0, ctx->stream>>>(a.terms, a.groups, a.outer_mask, ntiles,
+                                                          static_cast<double2*>(ctx->gv_buf.ptr));
             QSE_CUDA(cudaGetLastError());
             count_launch(ctx);
             gvt = ctx->gv_buf.ptr;
@@ -564,12 +565,28 @@ double adjoint(qse_state* st, const qse_op* ops, size_t nops, const double* para
     if (!st->aux) QSE_CUDA(cudaMalloc(&st->aux, st->size() * 16));
     double value = run_obs(st, obs, reinterpret_cast<double2*>(st->aux));
 
-    // reverse sweep over the inverse gates, gradient slots on parameterised ones
+    // reverse sweep over the inverse gates, gradient slots on parameterised ones.
+    // Slot sums give 2 Im<l|G|s> for X/Y/Z generators and -2 Im<l|P|s> must be
+    // applied for phase types (factor f); occurrences of one parameter with the
+    // same coeff * f add into one bucket, reduced once per pass
     std::vector<plan::Gate> rev;
     rev.reserve(nops);
+    std::map<std::pair<int32_t, double>, int32_t> bucket_of;
+    std::vector<std::pair<int32_t, double>> buckets;
     for (size_t i = nops; i-- > 0;) {
         double th = bound_angle(ops[i], params, nparams);
-        int32_t gid = (ops[i].param >= 0 && parameterised(ops[i].type)) ? int32_t(i) : -1;
+        int32_t gid = -1;
+        if (ops[i].param >= 0 && parameterised(ops[i].type)) {
+            const double f = (ops[i].type == QSE_GATE_PHASE || ops[i].type == QSE_GATE_CPHASE ||
+                              ops[i].type == QSE_GATE_MCPHASE) ? -2.0 : 1.0;
+            const std::pair<int32_t, double> key{ops[i].param, ops[i].coeff * f};
+            auto it = bucket_of.find(key);
+            if (it == bucket_of.end()) {
+                it = bucket_of.emplace(key, int32_t(buckets.size())).first;
+                buckets.push_back(key);
+            }
+            gid = it->second;
+        }
         rev.push_back(inverse_gate(ops[i], th, gid));
     }
     plan::Options opt;
@@ -624,13 +641,8 @@ double adjoint(qse_state* st, const qse_op* ops, size_t nops, const double* para
     QSE_CUDA(cudaMemcpyAsync(hocc.data(), occ, nops * 8, cudaMemcpyDeviceToHost, ctx->stream));
     QSE_CUDA(cudaStreamSynchronize(ctx->stream));
     for (size_t p = 0; p < nparams; ++p) grad[p] = 0.0;
-    for (size_t i = 0; i < nops; ++i) {
-        if (ops[i].param < 0 || !parameterised(ops[i].type)) continue;
-        // slot sums: X/Y/Z generators give 2 Im<l|G|s> directly; phase-type G = -P gives -2 Im<l|P|s>
-        double f = (ops[i].type == QSE_GATE_PHASE || ops[i].type == QSE_GATE_CPHASE ||
-                    ops[i].type == QSE_GATE_MCPHASE) ? -2.0 : 1.0;
-        grad[ops[i].param] += ops[i].coeff * f * hocc[i];
-    }
+    for (size_t b = 0; b < buckets.size(); ++b)
+        if (size_t(buckets[b].first) < nparams) grad[buckets[b].first] += buckets[b].second * hocc[b];
     return value;
 }
 

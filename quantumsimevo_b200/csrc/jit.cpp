@@ -98,6 +98,9 @@ struct Gen {
     int basis_slot = -1;    // prm slot of bi (set per launch)
     bool xb_used = false;   // the exchange buffer holds data some thread may still read
     std::string SYNC = "__syncthreads();";   // barrier of the threads that share xb
+    // gradient slots accumulated per thread (slot -> accumulator index)
+    static constexpr uint32_t kRegSlots = 4;
+    std::map<uint16_t, uint32_t> gacc;
     // the per-CTA group values come precomputed from global memory (gvt, one row
     // of ng values per tile): the prologue copies them instead of summing terms
     // and calling sincos per group
@@ -403,6 +406,9 @@ struct Gen {
             if (ns == 2) o << " lam[gb + " << hex(reg_off(j)) << "] = a1[" << j << "];";
             o << "\n";
         }
+        for (const auto& kv : gacc)
+            o << "  { const double v = warpSum<" << T << ">(gs" << kv.second << ");"
+              << " if ((tid & 31u) == 0u) wp[" << kv.first << "u * " << NW << "u + (tid >> 5)] += v; }\n";
         if (ns == 2 && nslots) {
             o << "  __syncthreads();\n"
               << "  for (u32 s = tid; s < " << nslots << "u; s += " << T << "u) { double v = 0.0;"
@@ -416,6 +422,7 @@ struct Gen {
         std::ostringstream head;
         std::swap(o, head);
         o << "  const u32 tid = threadIdx.x;\n";
+        for (const auto& kv : gacc) o << "  double gs" << kv.second << " = 0.0;\n";
         o << "  extern __shared__ double2 sm[];\n";
         o << "  double2* xb = sm; (void)xb;\n";
         o << "  double2* gv = sm + " << tsize << "; (void)gv;\n";
@@ -462,8 +469,7 @@ struct Gen {
         }
         // prologue: per-CTA diagonal group values, then the lane tables
         if (ng && pre_gv) {
-            o << "  for (u32 g = tid; g < " << ng << "u; g += " << T << "u) gv[g] = gvt[(u64)blockIdx.x * " << ng
-              << "u + g];\n";
+            o << "  for (u32 g = tid; g < " << ng << "u; g += " << T << "u) gv[g] = gvt[(u64)g * gridDim.x + blockIdx.x];\n";
         } else if (ng) {
             // the pass's terms are first copied into the exchange buffer (unused until
             // the first layout exchange, which follows the prologue's barrier) by every
@@ -756,8 +762,16 @@ struct Gen {
                 if (!c.empty()) expr = "((" + c + ") ? " + expr + " : 0.0)";
             }
             const uint32_t si = push(op.a);
-            o << "  { const double v = warpSum<" << T << ">(" << expr << " * P.v[" << si << "]);"
-              << " if ((tid & 31u) == 0u) wp[" << op.g << "u * " << NW << "u + (tid >> 5)] += v; }\n";
+            // the first kRegSlots slots of a pass accumulate in registers (one
+            // warp reduction per slot at the end of the pass instead of one per
+            // gate occurrence); further slots reduce immediately
+            auto it = gacc.find(op.g);
+            if (it == gacc.end() && gacc.size() < kRegSlots) it = gacc.emplace(op.g, uint32_t(gacc.size())).first;
+            if (it != gacc.end())
+                o << "  gs" << it->second << " += " << expr << " * P.v[" << si << "];\n";
+            else
+                o << "  { const double v = warpSum<" << T << ">(" << expr << " * P.v[" << si << "]);"
+                  << " if ((tid & 31u) == 0u) wp[" << op.g << "u * " << NW << "u + (tid >> 5)] += v; }\n";
             break;
         }
         default: break;

@@ -515,8 +515,13 @@ private:
         }
     }
 
+    // one slot per gradient source within a pass: occurrences that share a
+    // source (the adjoint gives occurrences of one parameter with one factor the
+    // same source) add into one slot
     uint16_t new_slot(int32_t src)
     {
+        for (size_t s = 0; s < P.slot_src.size(); ++s)
+            if (P.slot_src[s] == src) return uint16_t(s);
         P.slot_src.push_back(src);
         return uint16_t(P.slot_src.size() - 1);
     }
