@@ -114,20 +114,26 @@ size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
 struct Uploaded {
     std::vector<tile::PassArgs> args;
+    std::vector<const double2*> texp;   // per pass: (cos, sin) of each term's angle
 };
 
-// Packs every pass program into one pinned buffer and one H2D copy.
-Uploaded upload_plan(qse_ctx* ctx, const plan::Plan& pl)
+// Packs every pass program into one pinned buffer and one H2D copy.  With
+// term_phases, each pass also gets the (cos, sin) of its terms' angles (for
+// k_group_values; only passes whose kernels read precomputed group values).
+Uploaded upload_plan(qse_ctx* ctx, const plan::Plan& pl, bool term_phases = false)
 {
-    std::vector<size_t> off(pl.passes.size() * 5);
+    constexpr size_t kArr = 6;
+    std::vector<size_t> off(pl.passes.size() * kArr);
     size_t total = 0;
     for (size_t i = 0; i < pl.passes.size(); ++i) {
         const plan::PassProgram& p = pl.passes[i];
-        off[5 * i + 0] = total; total = align16(total + p.ops.size() * sizeof(plan::KOp));
-        off[5 * i + 1] = total; total = align16(total + p.layouts.size() * sizeof(plan::LayoutRec));
-        off[5 * i + 2] = total; total = align16(total + p.terms.size() * sizeof(plan::TermRec));
-        off[5 * i + 3] = total; total = align16(total + p.groups.size() * sizeof(plan::GroupRec));
-        off[5 * i + 4] = total; total = align16(total + p.mats.size() * sizeof(double));
+        size_t* o = &off[kArr * i];
+        o[0] = total; total = align16(total + p.ops.size() * sizeof(plan::KOp));
+        o[1] = total; total = align16(total + p.layouts.size() * sizeof(plan::LayoutRec));
+        o[2] = total; total = align16(total + p.terms.size() * sizeof(plan::TermRec));
+        o[3] = total; total = align16(total + p.groups.size() * sizeof(plan::GroupRec));
+        o[4] = total; total = align16(total + p.mats.size() * sizeof(double));
+        o[5] = total; total = align16(total + (term_phases ? p.terms.size() * sizeof(double2) : 0));
     }
     total = std::max<size_t>(total, 16);
     QSE_CUDA(cudaEventSynchronize(ctx->plan_event));
@@ -136,11 +142,16 @@ Uploaded upload_plan(qse_ctx* ctx, const plan::Plan& pl)
     char* h = static_cast<char*>(ctx->plan_host.ptr);
     for (size_t i = 0; i < pl.passes.size(); ++i) {
         const plan::PassProgram& p = pl.passes[i];
-        std::memcpy(h + off[5 * i + 0], p.ops.data(), p.ops.size() * sizeof(plan::KOp));
-        std::memcpy(h + off[5 * i + 1], p.layouts.data(), p.layouts.size() * sizeof(plan::LayoutRec));
-        std::memcpy(h + off[5 * i + 2], p.terms.data(), p.terms.size() * sizeof(plan::TermRec));
-        std::memcpy(h + off[5 * i + 3], p.groups.data(), p.groups.size() * sizeof(plan::GroupRec));
-        std::memcpy(h + off[5 * i + 4], p.mats.data(), p.mats.size() * sizeof(double));
+        const size_t* o = &off[kArr * i];
+        std::memcpy(h + o[0], p.ops.data(), p.ops.size() * sizeof(plan::KOp));
+        std::memcpy(h + o[1], p.layouts.data(), p.layouts.size() * sizeof(plan::LayoutRec));
+        std::memcpy(h + o[2], p.terms.data(), p.terms.size() * sizeof(plan::TermRec));
+        std::memcpy(h + o[3], p.groups.data(), p.groups.size() * sizeof(plan::GroupRec));
+        std::memcpy(h + o[4], p.mats.data(), p.mats.size() * sizeof(double));
+        double2* e = reinterpret_cast<double2*>(h + o[5]);
+        if (term_phases)
+            for (size_t t = 0; t < p.terms.size(); ++t)
+                e[t] = make_double2(std::cos(p.terms[t].theta), std::sin(p.terms[t].theta));
     }
     QSE_CUDA(cudaMemcpyAsync(ctx->plan_buf.ptr, h, total, cudaMemcpyHostToDevice, ctx->stream));
     QSE_CUDA(cudaEventRecord(ctx->plan_event, ctx->stream));
@@ -148,12 +159,14 @@ Uploaded upload_plan(qse_ctx* ctx, const plan::Plan& pl)
     Uploaded up;
     for (size_t i = 0; i < pl.passes.size(); ++i) {
         const plan::PassProgram& p = pl.passes[i];
+        const size_t* o = &off[kArr * i];
         tile::PassArgs a{};
-        a.ops = reinterpret_cast<const plan::KOp*>(d + off[5 * i + 0]);
-        a.layouts = reinterpret_cast<const plan::LayoutRec*>(d + off[5 * i + 1]);
-        a.terms = reinterpret_cast<const plan::TermRec*>(d + off[5 * i + 2]);
-        a.groups = reinterpret_cast<const plan::GroupRec*>(d + off[5 * i + 3]);
-        a.mats = reinterpret_cast<const double*>(d + off[5 * i + 4]);
+        a.ops = reinterpret_cast<const plan::KOp*>(d + o[0]);
+        a.layouts = reinterpret_cast<const plan::LayoutRec*>(d + o[1]);
+        a.terms = reinterpret_cast<const plan::TermRec*>(d + o[2]);
+        a.groups = reinterpret_cast<const plan::GroupRec*>(d + o[3]);
+        a.mats = reinterpret_cast<const double*>(d + o[4]);
+        up.texp.push_back(reinterpret_cast<const double2*>(d + o[5]));
         a.outer_mask = p.outer_mask;
         a.nops = uint32_t(p.ops.size());
         a.ngroups = uint32_t(p.groups.size());
@@ -166,35 +179,57 @@ Uploaded upload_plan(qse_ctx* ctx, const plan::Plan& pl)
     return up;
 }
 
-// The per-CTA values of a pass's diagonal groups, group-major (out[g * ntiles +
-// t]): group g of tile t sums the angles of its terms whose outer-qubit
+// The per-CTA values of a pass's diagonal groups, one row per tile (out[t * ng
+// + g], the row CTA t of the pass copies).  The value of a direct group is the
+// product of the unit phases (cos, sin) of its terms whose outer-qubit
 // conditions hold for t's outer bits (t's bits deposited on the outer positions
-// in ascending order, as the pass kernel numbers its CTAs), then (cos, sin) for
-// direct groups.  Same sums, in the same order, as the prologue a pass kernel
-// otherwise runs per CTA; here they run on the whole GPU ahead of the pass, so
-// the pass starts its arithmetic without a per-CTA sincos chain.  Grid: tiles
-// along x, groups along y (a group's terms are read by the whole warp at once).
+// in ascending order, as the pass kernel numbers its CTAs); each term's phase
+// is computed once on the host, so this kernel multiplies and never takes a
+// sincos.  Other groups keep the plain sum of their angles.  A CTA handles
+// kGvTiles consecutive tiles: their outer bits once into shared memory, then
+// its threads walk the rows' elements in address order (coalesced stores).
+constexpr uint32_t kGvTiles = 32;
+
 __global__ void __launch_bounds__(256) k_group_values(const plan::TermRec* __restrict__ terms,
-                                                      const plan::GroupRec* __restrict__ groups, uint64_t outer_mask,
-                                                      uint64_t ntiles, double2* __restrict__ out)
+                                                      const double2* __restrict__ texp,
+                                                      const plan::GroupRec* __restrict__ groups, uint32_t ng,
+                                                      uint64_t outer_mask, uint64_t ntiles, double2* __restrict__ out)
 {
-    const uint32_t g = blockIdx.y;
-    const plan::GroupRec gr = groups[g];
-    for (uint64_t tile = blockIdx.x * uint64_t(blockDim.x) + threadIdx.x; tile < ntiles;
-         tile += uint64_t(gridDim.x) * blockDim.x) {
-        uint64_t ob = 0, c = tile;
+    __shared__ uint64_t s_ob[kGvTiles];
+    const uint64_t t0 = uint64_t(blockIdx.x) * kGvTiles;
+    if (threadIdx.x < kGvTiles) {
+        uint64_t ob = 0, c = t0 + threadIdx.x;
         for (uint64_t m = outer_mask; m; m &= m - 1) {
             ob |= (c & 1ull) << (__ffsll((long long)m) - 1);
             c >>= 1;
         }
-        double th = 0.0;
-        for (uint32_t k = 0; k < gr.count; ++k) {
-            const plan::TermRec t = terms[gr.first + k];
-            if ((ob & t.ocond) == t.ocond) th += t.theta;
+        s_ob[threadIdx.x] = ob;
+    }
+    __syncthreads();
+    const uint32_t nt = uint32_t(min(uint64_t(kGvTiles), ntiles - t0));
+    const uint32_t cnt = nt * ng;
+    double2* row = out + t0 * ng;
+    for (uint32_t e = threadIdx.x; e < cnt; e += blockDim.x) {
+        const uint32_t tl = e / ng, g = e - tl * ng;
+        const uint64_t ob = s_ob[tl];
+        const plan::GroupRec gr = groups[g];
+        double2 v;
+        if (gr.direct) {
+            v = make_double2(1.0, 0.0);
+            for (uint32_t k = 0; k < gr.count; ++k)
+                if ((ob & terms[gr.first + k].ocond) == terms[gr.first + k].ocond) {
+                    const double2 f = texp[gr.first + k];
+                    v = make_double2(v.x * f.x - v.y * f.y, v.x * f.y + v.y * f.x);
+                }
+        } else {
+            double th = 0.0;
+            for (uint32_t k = 0; k < gr.count; ++k) {
+                const plan::TermRec t = terms[gr.first + k];
+                if ((ob & t.ocond) == t.ocond) th += t.theta;
+            }
+            v = make_double2(th, 0.0);
         }
-        double s, co;
-        if (gr.direct) sincos(th, &s, &co);
-        out[uint64_t(g) * ntiles + tile] = gr.direct ? make_double2(co, s) : make_double2(th, 0.0);
+        row[e] = v;
     }
 }
 
@@ -273,9 +308,10 @@ struct PassRunner {
             const uint64_t ntiles = uint64_t(1) << (st->n - kq[i]);
             const uint64_t cnt = ntiles * srcs[i].ngroups;
             ctx->gv_buf.reserve(cnt * sizeof(double2));
-            const dim3 grid(unsigned(std::min<uint64_t>((ntiles + 255) / 256, 65535)), srcs[i].ngroups);
-            k_group_values<<<grid, 256, 0, ctx->stream>>>(a.terms, a.groups, a.outer_mask, ntiles,
-                                                          static_cast<double2*>(ctx->gv_buf.ptr));
+            const uint64_t blocks = (ntiles + kGvTiles - 1) / kGvTiles;
+            k_group_values<<<unsigned(blocks), 256, 0, ctx->stream>>>(a.terms, up.texp[i], a.groups, srcs[i].ngroups,
+                                                                     a.outer_mask, ntiles,
+                                                                     static_cast<double2*>(ctx->gv_buf.ptr));
             QSE_CUDA(cudaGetLastError());
             count_launch(ctx);
             gvt = ctx->gv_buf.ptr;
@@ -369,7 +405,7 @@ void execute_program(qse_state* st, const qse_op* ops, size_t nops, const double
         std::vector<jit::Source> srcs;
         plan::Plan pl = plan_for(st, gates, opt, 1, use_jit, srcs);
         if (!use_jit) materialize(st);  // interpreter passes read the state
-        Uploaded up = upload_plan(ctx, pl);
+        Uploaded up = upload_plan(ctx, pl, use_jit && st->n >= jit::kPreGroupQubits);
         PassRunner runner(st, pl, up, 1, 4, use_jit, std::move(srcs));
         for (size_t i = 0; i < up.args.size(); ++i) runner.run(i, nullptr, nullptr);
         if (!up.args.empty()) st->lazy_basis = false;  // the first pass wrote every amplitude
@@ -598,7 +634,7 @@ double adjoint(qse_state* st, const qse_op* ops, size_t nops, const double* para
     bool use_jit = false;
     std::vector<jit::Source> srcs;
     plan::Plan pl = plan_for(st, rev, opt, 2, use_jit, srcs);
-    Uploaded up = upload_plan(ctx, pl);
+    Uploaded up = upload_plan(ctx, pl, use_jit && st->n >= jit::kPreGroupQubits);
 
     // occurrence gradients accumulate in scratch2: [nops] | slot partials
     size_t max_part = 0;

@@ -469,7 +469,7 @@ struct Gen {
         }
         // prologue: per-CTA diagonal group values, then the lane tables
         if (ng && pre_gv) {
-            o << "  for (u32 g = tid; g < " << ng << "u; g += " << T << "u) gv[g] = gvt[(u64)g * gridDim.x + blockIdx.x];\n";
+            o << "  for (u32 g = tid; g < " << ng << "u; g += " << T << "u) gv[g] = gvt[(u64)blockIdx.x * " << ng << "u + g];\n";
         } else if (ng) {
             // the pass's terms are first copied into the exchange buffer (unused until
             // the first layout exchange, which follows the prologue's barrier) by every

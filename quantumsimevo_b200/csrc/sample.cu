@@ -745,6 +745,9 @@ __global__ void __launch_bounds__(kBT) k_cdf_summ(const double* __restrict__ pro
     if (threadIdx.x == blockDim.x - 1) summ[blockIdx.x] = out;
 }
 
+// blocks composed per thread in one step of the chain's fast path
+constexpr int kChainPer = 16;
+
 // single CTA: exact running sum block by block; blocks whose guess does not
 // hold are folded exactly here.  cin[b] = exact sum before block b; cin[nb] = total.
 __global__ void __launch_bounds__(kBT) k_cdf_chain(const double* __restrict__ prob,
@@ -768,23 +771,23 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double* __restrict__ pr
     __shared__ int s_end;
     uint32_t base = 0;
     while (base < nb) {
-        // Super-chunk of 4 kBT blocks, 4 consecutive per thread, taken whole
-        // when every block has a fold on the running sum's binade and the sum
-        // stays in it (nearly always); else the chunks below redo it.
-        if (base + 4 * kBT <= nb) {
+        // Super-chunk of kChainPer kBT blocks, kChainPer consecutive per thread,
+        // taken whole when every block has a fold on the running sum's binade
+        // and the sum stays in it (nearly always); else the chunks below redo it.
+        if (base + kChainPer * kBT <= nb) {
             const double c = s_c;
             const int e0 = epoch_of(c);
-            uint64_t d0[4], d1[4];
+            uint64_t d0[kChainPer], d1[kChainPer];
             bool good = c > 0.0;
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
+            for (int k = 0; k < kChainPer; ++k) {
                 d0[k] = d1[k] = 0;
-                good = summ_pick(summ[base + 4 * t + k], e0, d0[k], d1[k]) && good;
+                good = summ_pick(summ[base + kChainPer * t + k], e0, d0[k], d1[k]) && good;
             }
             if (__syncthreads_and(good)) {
                 uint64_t m0 = 0, m1 = 0;
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
+                for (int k = 0; k < kChainPer; ++k) {
                     uint64_t r0, r1;
                     compose(m0, m1, d0[k], d1[k], r0, r1);
                     m0 = r0;
@@ -799,19 +802,19 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double* __restrict__ pr
                 }
                 const uint64_t C = uint64_t(ldexp(c, 52 - e0));
                 uint64_t x = C + ((C & 1) ? ex1 : ex0);
-                uint64_t xin[4];
+                uint64_t xin[kChainPer];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
+                for (int k = 0; k < kChainPer; ++k) {
                     xin[k] = x;
                     x += (x & 1) ? d1[k] : d0[k];
                 }
                 if (!__syncthreads_or(x >= kTwo53)) {   // sums only grow: the last is the largest
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) cin[base + 4 * t + k] = ldexp(double(xin[k]), e0 - 52);
+                    for (int k = 0; k < kChainPer; ++k) cin[base + kChainPer * t + k] = ldexp(double(xin[k]), e0 - 52);
                     if (t == kBT - 1) s_c = ldexp(double(x), e0 - 52);
                     ++n_fast;
                     __syncthreads();
-                    base += 4 * kBT;
+                    base += kChainPer * kBT;
                     continue;
                 }
             }
