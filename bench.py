@@ -38,8 +38,10 @@ batch      512 parameterised circuits (widths 10..22): forward <O> and the full
            kernels.  --batch-only runs just this section (--batch-circuits/
            -wmin/-wmax set a smaller case, --no-autotune keeps the default
            configuration).
-Multi-GPU: the state does not shard here; every rank runs its own replica
-(weak scaling), value = sum over ranks.
+Multi-GPU: the step's state does not shard; every rank runs its own replica
+(weak scaling), value = sum over ranks.  --sharded QUBITS instead runs one
+state of QUBITS qubits sharded over the N ranks (strong scaling, execute only,
+NCCL half-shard exchanges) and prints that line.
 """
 from __future__ import annotations
 
@@ -87,6 +89,9 @@ def parse():
     ap.add_argument("--pass-kernel", type=int, default=-1, choices=[-1, 0, 1, 2],
                     help="pass kernels (qse_ctx_set_jit): 0 interpreter, 1 one CTA per tile, 2 streamed; "
                          "-1 = library default")
+    ap.add_argument("--sharded", type=int, default=0, metavar="QUBITS",
+                    help="instead of the step: one H+RZ+QFT state of QUBITS qubits sharded over the N ranks "
+                         "(2^g = N, the top g qubits global; NCCL half-shard exchanges), execute only")
     ap.add_argument("--playground", default=None,
                     help="comma-separated playground workloads (or 'all'): the paper's construct -> execute -> "
                          "sample wall-clock timings, one JSON line instead of the step")
@@ -458,6 +463,14 @@ def main():
             dist.destroy_process_group()
         return
 
+    if args.sharded:
+        r = bench_sharded(args, dist, rank, world, local, L, W, np)
+        if rank == 0:
+            print(json.dumps(r))
+        if dist:
+            dist.destroy_process_group()
+        return
+
     if args.batch_only:
         r = bench_batch(Device(local), L, W, np, steps=args.steps, warmup=args.warmup,
                         autotune=not args.no_autotune, count=args.batch_circuits, wmin=args.batch_wmin,
@@ -652,6 +665,72 @@ def main():
         print(json.dumps(line))
     if dist:
         dist.destroy_process_group()
+
+
+def bench_sharded(args, dist, rank, world, local, L, W, np):
+    """One n-qubit H+RZ+QFT state over the N ranks (quantumsimevo_b200.sharded):
+    each step resets the shards and executes the 540-gate circuit (at 30
+    qubits; 18n gates in general), local segments as fused passes on each
+    rank's engine, global-qubit gates through pipelined half-shard exchanges
+    with the partner rank.  Total work is fixed as N grows (strong scaling).
+    Timed from a barrier to a barrier with the host clock (the exchanges
+    synchronise the host with both the engine stream and NCCL), max over ranks."""
+    import torch
+
+    from quantumsimevo_b200 import sharded as S
+    from quantumsimevo_b200.circuit import Device
+    n = args.sharded
+    g = world.bit_length() - 1
+    if (1 << g) != world or n - g < 12:
+        raise SystemExit("--sharded needs a power-of-two rank count and at least 12 local qubits")
+    ops = W.hrz_qft(n, seed=2)
+    dev = Device(local)
+    shard = S.DeviceShard(n - g, rank, dev)
+    stats = {}
+
+    def step(st):
+        shard.reset()
+        S.execute_rank(ops, n, g, rank, shard, dist, stats=st)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+
+    for _ in range(args.warmup):
+        step(None)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step(stats)
+    barrier()
+    sec = (time.perf_counter() - t0) / args.steps
+    if dist:
+        t = torch.tensor([sec, stats.get("exchange_s", 0.0) / args.steps], dtype=torch.float64,
+                         device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sec, exch = float(t[0]), float(t[1])
+    else:
+        exch = stats.get("exchange_s", 0.0) / args.steps
+    nex = stats.get("exchanges", 0) / args.steps
+    xbytes = stats.get("exchange_bytes", 0) / args.steps
+    del shard
+    return {
+        "metric": f"sharded {n}q H+RZ+QFT execute gates/s", "value": len(ops) / sec, "unit": "gates/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"H+RZ+QFT {n}q complex128 ({len(ops)} gates), one state over {world} ranks",
+                   "qubits": n, "gates": len(ops), "global_qubits": g,
+                   "l2": f"shard ({16 << (n - g) >> 20} MiB per rank) streamed from HBM by every pass"},
+        "parallelism": f"sharded{world}",
+        "exchanges_per_execute": nex,
+        "exchange_ms": exch * 1e3,
+        "exchange_bytes_sent_per_rank": xbytes,
+        "exchange_gbs_per_rank": (xbytes / exch / 1e9) if exch > 0 else None,
+        "nvlink_peer_copy_gbs": 770.0,
+        "timing": "host clock between barriers (every exchange synchronises the host with the engine stream "
+                  "and NCCL), max over ranks; exchange_ms: host time inside the exchanges",
+    }
 
 
 def bench_playground(dev, names):

@@ -663,17 +663,27 @@ constexpr size_t kStage2 = size_t(2) * kBT * kPad * sizeof(double);
 // the persistent grid is exactly that many per SM
 constexpr int kWriteCTAs = 2;
 
-// fold of one block on the one or two binades its guess allows
-__device__ __forceinline__ Summ block_summ(const double (&p)[kEPT], int32_t gs, uint64_t* sh)
+// Fold of one block on the one or two binades its guess allows.  p holds the
+// block coalesced (p[j] = element j * kBT + tid).  Per binade, three facts are
+// independent of the element order: whether an element leaves the binade by
+// itself (no fold there), whether any element lands on a tie of the grid, and
+// the integer sum of the rounded elements.  Without ties every element's map
+// is a translation, so the fold is that sum (exact below 2^53, and a sum at or
+// above 2^53 stays there under rounding: the block then leaves the binade).
+// Only a binade with a tie composes the maps in element order, after the block
+// is restaged so that thread tid holds elements tid * kEPT .. + kEPT - 1.
+__device__ __forceinline__ Summ block_summ(const double (&p)[kEPT], int32_t gs, uint64_t* sh, double* stage)
 {
     const int32_t e = gs >> 1;          // arithmetic shift: floor(gs / 2)
     const int nbin = 1 + (gs & 1);      // binades the block may run in
     Summ out{{{0, 0}, {0, 0}}, e, 0};
+    unsigned flags = 0;                 // bit 2k: every element stays in binade e+k; bit 2k+1: no tie there
+    double tsum[2] = {0.0, 0.0};
     for (int k = 0; k < nbin; ++k) {
         const Grid g = grid_of(e + k);
         int ok = 1;
         bool pure = true;
-        double tsum = 0.0;
+        double t = 0.0;
         if (g.fast) {
             // grid integers as doubles (exact below 2^53; a larger total
             // means the block leaves the binade, whatever its exact value)
@@ -684,7 +694,7 @@ __device__ __forceinline__ Summ block_summ(const double (&p)[kEPT], int32_t gs, 
                 const double df = x - r;
                 if (!(p[j] < g.limit)) ok = 0;
                 pure = pure && df != 0.5 && df != -0.5;
-                tsum += r;
+                t += r;
             }
         } else {
 #pragma unroll
@@ -692,27 +702,56 @@ __device__ __forceinline__ Summ block_summ(const double (&p)[kEPT], int32_t gs, 
                 uint64_t a0, a1;
                 if (!elem_map_g(p[j], g, a0, a1)) ok = 0;
                 pure = pure && a0 == a1;
-                tsum += double(a0);
+                t += double(a0);
             }
         }
-        const int both = __syncthreads_and(ok) | (__syncthreads_and(pure) << 1);
-        if (!(both & 1)) continue;  // an element leaves binade e+k by itself: no fold there
-        if (both & 2) {
-            double* shd = reinterpret_cast<double*>(sh);
-            for (int o = 16; o > 0; o >>= 1) tsum += __shfl_xor_sync(0xffffffffu, tsum, o);
-            if ((threadIdx.x & 31) == 0) shd[threadIdx.x >> 5] = tsum;
-            __syncthreads();
-            double total = 0.0;
-            for (int w = 0; w < kBT / 32; ++w) total += shd[w];
-            __syncthreads();
-            const uint64_t d = total >= 0x1p53 ? kTwo53 : uint64_t(total);
+        flags |= unsigned(ok) << (2 * k) | unsigned(pure) << (2 * k + 1);
+        tsum[k] = t;
+    }
+    // one barrier for the flags of both binades and both sums
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    flags = __reduce_and_sync(0xffffffffu, flags);
+    for (int o = 16; o > 0; o >>= 1) {
+        tsum[0] += __shfl_xor_sync(0xffffffffu, tsum[0], o);
+        tsum[1] += __shfl_xor_sync(0xffffffffu, tsum[1], o);
+    }
+    double* shd = reinterpret_cast<double*>(sh);
+    if (lane == 0) {
+        shd[warp] = tsum[0];
+        shd[kBT / 32 + warp] = tsum[1];
+        sh[2 * (kBT / 32) + warp] = flags;
+    }
+    __syncthreads();
+    double total[2] = {0.0, 0.0};
+    unsigned all = ~0u;
+    for (int w = 0; w < kBT / 32; ++w) {
+        total[0] += shd[w];
+        total[1] += shd[kBT / 32 + w];
+        all &= unsigned(sh[2 * (kBT / 32) + w]);
+    }
+    __syncthreads();   // sh is reused below
+    bool staged = false;
+    double q[kEPT];
+    for (int k = 0; k < nbin; ++k) {
+        if (!((all >> (2 * k)) & 1)) continue;  // an element leaves binade e+k by itself: no fold there
+        if ((all >> (2 * k + 1)) & 1) {
+            const uint64_t d = total[k] >= 0x1p53 ? kTwo53 : uint64_t(total[k]);
             out.d[k][0] = out.d[k][1] = d;
         } else {
+            if (!staged) {
+#pragma unroll
+                for (int j = 0; j < kEPT; ++j) stage[stage_slot(j * kBT + threadIdx.x)] = p[j];
+                __syncthreads();
+#pragma unroll
+                for (int j = 0; j < kEPT; ++j) q[j] = stage[threadIdx.x * kPad + j];
+                staged = true;
+            }
+            const Grid g = grid_of(e + k);
             uint64_t t0 = 0, t1 = 0;
 #pragma unroll
             for (int j = 0; j < kEPT; ++j) {
                 uint64_t a0, a1, r0, r1;
-                elem_map_g(p[j], g, a0, a1);
+                elem_map_g(q[j], g, a0, a1);
                 compose(t0, t1, a0, a1, r0, r1);
                 t0 = r0;
                 t1 = r1;
@@ -729,6 +768,8 @@ __device__ __forceinline__ Summ block_summ(const double (&p)[kEPT], int32_t gs, 
     return out;
 }
 
+// One CTA per block: the block's probabilities straight into registers
+// (coalesced, no staging unless a binade has a tie), then its fold.
 __global__ void __launch_bounds__(kBT) k_cdf_summ(const double* __restrict__ prob,
                                                   const int32_t* __restrict__ guess, Summ* __restrict__ summ)
 {
@@ -739,156 +780,139 @@ __global__ void __launch_bounds__(kBT) k_cdf_summ(const double* __restrict__ pro
         return;
     }
     __shared__ double stage[kBT * kPad];
+    const double* src = prob + uint64_t(blockIdx.x) * kBS + threadIdx.x;
     double p[kEPT];
-    load_block_prob(prob, uint64_t(blockIdx.x) * kBS, p, stage);
-    const Summ out = block_summ(p, gs, sh);
+#pragma unroll
+    for (int j = 0; j < kEPT; ++j) p[j] = src[j * kBT];
+    const Summ out = block_summ(p, gs, sh, stage);
     if (threadIdx.x == blockDim.x - 1) summ[blockIdx.x] = out;
 }
 
-// blocks composed per thread in one step of the chain's fast path
+// blocks composed per thread in one step of the chain
 constexpr int kChainPer = 16;
 
-// single CTA: exact running sum block by block; blocks whose guess does not
-// hold are folded exactly here.  cin[b] = exact sum before block b; cin[nb] = total.
+// Single CTA: the exact running sum block by block.  cin[b] = exact sum
+// before block b; cin[nb] = total.  A running sum of zero is on the grid of
+// binade -1022 (spacing 2^-1074, shared by the subnormals), where zero and
+// subnormal blocks fold exactly, so leading zero blocks take the fast path.  Each step takes the next span of up to
+// kChainPer * kBT blocks (kChainPer consecutive per thread): every block up to
+// the first one without a fold on the running sum's binade composes with one
+// block-wide scan, and the step commits the blocks up to the first one whose
+// sum would leave the binade (or the one without a fold).  That block is
+// handled on its own (its fold on the binade it actually starts in, else an
+// exact element-by-element fold) and the next span starts after it, so every
+// step advances past every block it could commit.
 __global__ void __launch_bounds__(kBT) k_cdf_chain(const double* __restrict__ prob,
                                                    const Summ* __restrict__ summ, uint32_t nb, double* __restrict__ cin,
                                                    uint32_t* __restrict__ stats)
 {
     __shared__ uint64_t sh[160];
     __shared__ double stage[kBT * kPad];
-    uint32_t n_fast = 0, n_slow = 0, n_exact = 0;  // chunk / block statistics (thread 0)
     __shared__ double s_c;
     __shared__ int s_slow;
+    __shared__ uint32_t s_end;
+    uint32_t n_span = 0, n_single = 0, n_exact = 0;  // statistics (thread 0)
     const uint32_t t = threadIdx.x;
     if (t == 0) s_c = 0.0;
     __syncthreads();
-    // Chunks of kBT consecutive blocks.  From position pos, the blocks whose
-    // fold exists on the grid of the running sum's binade compose with one
-    // block-wide scan up to the first block that has no such fold or whose
-    // sum leaves the binade; that block is handled on its own (its fold on
-    // the binade it actually starts in, else an exact element-by-element
-    // fold) and the scan restarts after it.
-    __shared__ int s_end;
     uint32_t base = 0;
     while (base < nb) {
-        // Super-chunk of kChainPer kBT blocks, kChainPer consecutive per thread,
-        // taken whole when every block has a fold on the running sum's binade
-        // and the sum stays in it (nearly always); else the chunks below redo it.
-        if (base + kChainPer * kBT <= nb) {
-            const double c = s_c;
-            const int e0 = epoch_of(c);
-            uint64_t d0[kChainPer], d1[kChainPer];
-            bool good = c > 0.0;
+        const double c = s_c;
+        const int e0 = epoch_of(c);
+        const uint32_t span = min(uint32_t(kChainPer * kBT), nb - base);
+        const uint32_t p0 = t * kChainPer;           // this thread's first position in the span
+        uint64_t d0[kChainPer], d1[kChainPer];
+        uint32_t my_bad = span;
 #pragma unroll
-            for (int k = 0; k < kChainPer; ++k) {
-                d0[k] = d1[k] = 0;
-                good = summ_pick(summ[base + kChainPer * t + k], e0, d0[k], d1[k]) && good;
-            }
-            if (__syncthreads_and(good)) {
-                uint64_t m0 = 0, m1 = 0;
-#pragma unroll
-                for (int k = 0; k < kChainPer; ++k) {
-                    uint64_t r0, r1;
-                    compose(m0, m1, d0[k], d1[k], r0, r1);
-                    m0 = r0;
-                    m1 = r1;
-                }
-                uint64_t ex0, ex1;
-                if (__syncthreads_and(m0 == m1)) {
-                    block_scan_add(m0, ex0, sh);
-                    ex1 = ex0;
-                } else {
-                    block_scan_maps(m0, m1, ex0, ex1, sh);
-                }
-                const uint64_t C = uint64_t(ldexp(c, 52 - e0));
-                uint64_t x = C + ((C & 1) ? ex1 : ex0);
-                uint64_t xin[kChainPer];
-#pragma unroll
-                for (int k = 0; k < kChainPer; ++k) {
-                    xin[k] = x;
-                    x += (x & 1) ? d1[k] : d0[k];
-                }
-                if (!__syncthreads_or(x >= kTwo53)) {   // sums only grow: the last is the largest
-#pragma unroll
-                    for (int k = 0; k < kChainPer; ++k) cin[base + kChainPer * t + k] = ldexp(double(xin[k]), e0 - 52);
-                    if (t == kBT - 1) s_c = ldexp(double(x), e0 - 52);
-                    ++n_fast;
-                    __syncthreads();
-                    base += kChainPer * kBT;
-                    continue;
-                }
-            }
+        for (int k = 0; k < kChainPer; ++k) {
+            d0[k] = d1[k] = 0;
+            const uint32_t pos = p0 + k;
+            if (pos < span && !summ_pick(summ[base + pos], e0, d0[k], d1[k]) && my_bad == span)
+                my_bad = pos;
         }
-        const uint32_t cnt = min(uint32_t(kBT), nb - base);
-        uint32_t pos = 0;
-        while (pos < cnt) {
-            const double c = s_c;
-            const int e0 = epoch_of(c);
-            uint64_t m0 = 0, m1 = 0;
-            bool good = true;
-            if (t >= pos && t < cnt) good = c > 0.0 && summ_pick(summ[base + t], e0, m0, m1);
-            if (t == 0) s_end = int(cnt);
-            __syncthreads();
-            if (!good) atomicMin(&s_end, int(t));
-            __syncthreads();
-            const uint32_t bad = uint32_t(s_end);
-            if (t >= bad) m0 = m1 = 0;
-            uint64_t ex0, ex1;
-            if (__syncthreads_and(m0 == m1)) {
-                block_scan_add(m0, ex0, sh);    // translations only: the prefix is a sum
-                ex1 = ex0;
-            } else {
-                block_scan_maps(m0, m1, ex0, ex1, sh);
-            }
-            const uint64_t C = c > 0.0 ? uint64_t(ldexp(c, 52 - e0)) : 0;
-            const uint64_t cin_t = C + ((C & 1) ? ex1 : ex0);
-            const uint64_t cout_t = cin_t + ((cin_t & 1) ? m1 : m0);
-            if (t == 0) s_end = int(bad);
-            __syncthreads();
-            if (t >= pos && t < bad && cout_t >= kTwo53) atomicMin(&s_end, int(t));
-            __syncthreads();
-            const uint32_t end = uint32_t(s_end);
-            if (t >= pos && t < end) cin[base + t] = ldexp(double(cin_t), e0 - 52);
-            if (end > pos && t == end - 1) s_c = ldexp(double(cout_t), e0 - 52);
-            if (end > pos) ++n_fast;
-            __syncthreads();
-            if (end >= cnt) break;
-            ++n_slow;
-            const uint32_t b = base + end;
-            pos = end + 1;
-            if (t == 0) {
-                double cc = s_c;
-                cin[b] = cc;
-                const int eb = epoch_of(cc);
-                uint64_t b0, b1;
-                int slow = 1;
-                if (cc > 0.0 && summ_pick(summ[b], eb, b0, b1)) {
-                    uint64_t Cb = uint64_t(ldexp(cc, 52 - eb));
-                    uint64_t Co = Cb + ((Cb & 1) ? b1 : b0);
-                    if (Co < kTwo53 && Co >= Cb) {
-                        s_c = ldexp(double(Co), eb - 52);
-                        slow = 0;
-                    }
-                }
-                s_slow = slow;
-            }
-            __syncthreads();
-            if (s_slow) {
-                ++n_exact;
-                double p[kEPT];
-                load_block_prob(prob, uint64_t(b) * kBS, p, stage);
-                double cc = block_exact(kBS, s_c, nullptr, sh, stage);
-                if (t == 0) s_c = cc;
-            }
-            __syncthreads();
+        if (t == 0) s_end = span;
+        __syncthreads();
+        if (my_bad < span) atomicMin(&s_end, my_bad);
+        __syncthreads();
+        const uint32_t bad = s_end;
+        uint64_t m0 = 0, m1 = 0;
+#pragma unroll
+        for (int k = 0; k < kChainPer; ++k) {
+            if (p0 + k >= bad) d0[k] = d1[k] = 0;     // identity beyond the first block without a fold
+            uint64_t r0, r1;
+            compose(m0, m1, d0[k], d1[k], r0, r1);
+            m0 = r0;
+            m1 = r1;
         }
-        base += kBT;
+        uint64_t ex0, ex1;
+        if (__syncthreads_and(m0 == m1)) {
+            block_scan_add(m0, ex0, sh);    // translations only: the prefix is a sum
+            ex1 = ex0;
+        } else {
+            block_scan_maps(m0, m1, ex0, ex1, sh);
+        }
+        const uint64_t C = c > 0.0 ? uint64_t(ldexp(c, 52 - e0)) : 0;
+        uint64_t x = C + ((C & 1) ? ex1 : ex0);
+        uint64_t xin[kChainPer];
+        uint32_t my_over = bad;
+#pragma unroll
+        for (int k = 0; k < kChainPer; ++k) {
+            xin[k] = x;
+            x += (x & 1) ? d1[k] : d0[k];
+            if (x >= kTwo53 && my_over == bad && p0 + k < bad) my_over = p0 + k;   // the sum leaves the binade here
+        }
+        if (t == 0) s_end = bad;
+        __syncthreads();
+        if (my_over < bad) atomicMin(&s_end, my_over);
+        __syncthreads();
+        const uint32_t end = s_end;
+#pragma unroll
+        for (int k = 0; k < kChainPer; ++k) {
+            const uint32_t pos = p0 + k;
+            if (pos < end) cin[base + pos] = ldexp(double(xin[k]), e0 - 52);
+            if (pos + 1 == end) s_c = ldexp(double(xin[k] + ((xin[k] & 1) ? d1[k] : d0[k])), e0 - 52);
+        }
+        if (t == 0 && end > 0) ++n_span;
+        __syncthreads();
+        if (end >= span) {
+            base += span;
+            continue;
+        }
+        // block b starts in the running sum's binade but has no fold there or leaves it
+        ++n_single;
+        const uint32_t b = base + end;
+        if (t == 0) {
+            double cc = s_c;
+            cin[b] = cc;
+            const int eb = epoch_of(cc);
+            uint64_t b0, b1;
+            int slow = 1;
+            if (summ_pick(summ[b], eb, b0, b1)) {
+                uint64_t Cb = cc > 0.0 ? uint64_t(ldexp(cc, 52 - eb)) : 0;
+                uint64_t Co = Cb + ((Cb & 1) ? b1 : b0);
+                if (Co < kTwo53 && Co >= Cb) {
+                    s_c = ldexp(double(Co), eb - 52);
+                    slow = 0;
+                }
+            }
+            s_slow = slow;
+        }
+        __syncthreads();
+        if (s_slow) {
+            ++n_exact;
+            double p[kEPT];
+            load_block_prob(prob, uint64_t(b) * kBS, p, stage);
+            double cc = block_exact(kBS, s_c, nullptr, sh, stage);
+            if (t == 0) s_c = cc;
+        }
+        __syncthreads();
+        base = b + 1;
     }
     if (t == 0) {
         cin[nb] = s_c;
         if (stats) {
-            stats[0] = n_fast;
-            stats[1] = n_slow;
+            stats[0] = n_span;
+            stats[1] = n_single;
             stats[2] = n_exact;
             stats[3] = nb;
         }

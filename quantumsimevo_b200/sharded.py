@@ -217,32 +217,85 @@ class LocalTransport:
             b[:, 0, :] = tmp
 
 
+def exchange_pieces(rows: int, cols: int, chunk: int):
+    """The exchanged half (rows x cols amplitudes, rows of cols contiguous
+    amplitudes) cut into pieces of at most `chunk` amplitudes, in address
+    order: (row0, nrows, col0, ncols).  Whole rows go together while a row fits
+    in a chunk; longer rows are cut.  Both partners derive the same pieces."""
+    chunk = max(1, chunk)
+    if cols <= chunk:
+        per = chunk // cols
+        return [(r, min(per, rows - r), 0, cols) for r in range(0, rows, per)]
+    return [(r, 1, c, min(chunk, cols - c)) for r in range(rows) for c in range(0, cols, chunk)]
+
+
 class TorchDistTransport:
     """One shard per rank (a complex128 torch tensor); the exchange is a send and a
     receive of half the shard with the partner rank over torch.distributed (NCCL
-    between GPUs, gloo on CPU), carried as float64 pairs so every backend takes it."""
+    between GPUs, gloo on CPU), carried as float64 pairs so every backend takes it.
 
-    def __init__(self, tensor, rank: int, dist, group=None):
+    The half travels in pieces of at most `chunk_bytes`, pipelined: piece k+1 is
+    packed (when it is not one contiguous run) and posted before piece k is
+    waited for and copied into place, so under NCCL the transfer of one piece
+    overlaps the local copies of its neighbours on the compute stream, and the
+    staging memory is four pieces instead of two half-shards.  A piece's place
+    is overwritten only after its own send completed (its wait precedes the
+    copy), and the buffers of piece k are reused by piece k+2 only after piece
+    k's copy, which follows its wait."""
+
+    def __init__(self, tensor, rank: int, dist, group=None, chunk_bytes: int = 256 << 20):
         self.t = tensor
         self.rank = rank
         self.dist = dist
         self.group = group
+        self.chunk = max(1, chunk_bytes // 16)
+        self._send = [None, None]
+        self._recv = [None, None]
+
+    def _buf(self, which, slot, n):
+        import torch
+        bufs = self._send if which == 0 else self._recv
+        if bufs[slot] is None or bufs[slot].numel() < n:
+            bufs[slot] = torch.empty(min(self.chunk, self.t.numel()), dtype=self.t.dtype, device=self.t.device)
+        return bufs[slot][:n]
 
     def exchange(self, j: int, l: int, nl: int):
         import torch
         b = (self.rank >> j) & 1
         partner = self.rank ^ (1 << j)
-        x = self.t.view(1 << (nl - l - 1), 2, 1 << l)
-        send = torch.view_as_real(x[:, 1 - b, :].contiguous())
-        recv = torch.empty_like(send)
-        # one grouped send+receive: under NCCL both partners' sends and receives
-        # are posted together (a send issued alone would wait for a receive that
-        # sits queued behind the partner's own send on the same stream)
-        ops = [self.dist.P2POp(self.dist.isend, send, partner, group=self.group),
-               self.dist.P2POp(self.dist.irecv, recv, partner, group=self.group)]
-        for rq in self.dist.batch_isend_irecv(ops):
-            rq.wait()
-        x[:, 1 - b, :] = torch.view_as_complex(recv)
+        rows, cols = 1 << (nl - l - 1), 1 << l
+        half = self.t.view(rows, 2, cols)[:, 1 - b, :]
+        pieces = exchange_pieces(rows, cols, self.chunk)
+
+        def view(k):
+            r0, nr, c0, nc = pieces[k]
+            return half[r0:r0 + nr, c0:c0 + nc]
+
+        def post(k):
+            src = view(k)
+            n = src.numel()
+            if src.is_contiguous():
+                s = src.reshape(-1)
+            else:
+                s = self._buf(0, k & 1, n)
+                s.view(src.shape).copy_(src)
+            r = self._buf(1, k & 1, n)
+            # one grouped send+receive: under NCCL both partners' sends and
+            # receives are posted together (a send issued alone would wait for
+            # a receive that sits queued behind the partner's own send)
+            ops = [self.dist.P2POp(self.dist.isend, torch.view_as_real(s), partner, group=self.group),
+                   self.dist.P2POp(self.dist.irecv, torch.view_as_real(r), partner, group=self.group)]
+            return self.dist.batch_isend_irecv(ops), r
+
+        pending = post(0)
+        for k in range(len(pieces)):
+            nxt = post(k + 1) if k + 1 < len(pieces) else None
+            reqs, r = pending
+            for rq in reqs:
+                rq.wait()
+            dst = view(k)
+            dst.copy_(r.view(dst.shape))
+            pending = nxt
 
 
 def run_rank(steps, nl: int, execute, transport):
@@ -290,9 +343,19 @@ class DeviceShard:
         from .circuit import Device, StateVector
         self.device = device or Device.default()
         self.nl = nl
+        self.rank = rank
         self.sv = StateVector(nl, self.device)
         self.torch_device = torch.device("cuda", self.device.index)
-        if rank != 0:
+        self.reset()
+
+    def reset(self):
+        """The shard of |0..0>: rank 0 holds |0..0> of its local qubits (recorded,
+        not written: the next execute's first pass generates it), every other
+        rank zeros."""
+        import torch
+        if self.rank == 0:
+            L.check(L.lib.qse_state_reset(self.sv.handle))
+        else:
             self.tensor().zero_()
             torch.cuda.synchronize(self.torch_device)
 
@@ -316,27 +379,44 @@ class DeviceShard:
 
 class _Synced:
     """Wraps a transport: the engine's stream finishes before an exchange, the
-    exchange's torch work finishes before the engine's next launch."""
+    exchange's torch work finishes before the engine's next launch.  The
+    transport is built at the first exchange (a shard's device view writes a
+    recorded |0..0> out, which an execute with no exchange never needs).
+    stats, if given, accumulates "exchanges", "exchange_s" (host wall time
+    between the two synchronisations) and "exchange_bytes" (sent per rank)."""
 
-    def __init__(self, inner, shards):
-        self.inner = inner
+    def __init__(self, make_inner, shards, stats=None):
+        self.make_inner = make_inner
+        self.inner = None
         self.shards = shards
+        self.stats = stats
 
     def exchange(self, j, l, nl):
+        import time
+
         import torch
+        if self.inner is None:
+            self.inner = self.make_inner()
         for s in self.shards:
             s.synchronize()
+        t0 = time.perf_counter()
         self.inner.exchange(j, l, nl)
         for s in self.shards:
             torch.cuda.synchronize(s.torch_device)
+        if self.stats is not None:
+            self.stats["exchanges"] = self.stats.get("exchanges", 0) + 1
+            self.stats["exchange_s"] = self.stats.get("exchange_s", 0.0) + time.perf_counter() - t0
+            self.stats["exchange_bytes"] = self.stats.get("exchange_bytes", 0) + 8 * (1 << nl)
 
 
-def execute_rank(ops, n: int, g: int, rank: int, shard: DeviceShard, dist, params=None, group=None):
+def execute_rank(ops, n: int, g: int, rank: int, shard: DeviceShard, dist, params=None, group=None, stats=None,
+                 chunk_bytes: int = 256 << 20):
     """This rank's part of executing ops on the sharded n-qubit state (one
     process per GPU, torch.distributed already initialised; NCCL between
-    GPUs).  Returns the final logical -> physical qubit map."""
+    GPUs).  Returns the final logical -> physical qubit map.  stats: see
+    _Synced; chunk_bytes: the exchange's piece size (TorchDistTransport)."""
     steps, pos = lower(ops, n, g, rank, params)
-    tr = _Synced(TorchDistTransport(shard.tensor(), rank, dist, group), [shard])
+    tr = _Synced(lambda: TorchDistTransport(shard.tensor(), rank, dist, group, chunk_bytes), [shard], stats)
     run_rank(steps, n - g, shard.execute, tr)
     shard.synchronize()
     return pos
@@ -350,7 +430,7 @@ def execute_shards(ops, n: int, g: int, shards, params=None):
     for r in range(len(shards)):
         steps, pos = lower(ops, n, g, r, params)
         progs.append(steps)
-    tr = _Synced(LocalTransport([s.tensor() for s in shards]), shards)
+    tr = _Synced(lambda: LocalTransport([s.tensor() for s in shards]), shards)
     run_shards(progs, n - g, lambda r, o: shards[r].execute(o), tr)
     for s in shards:
         s.synchronize()

@@ -268,6 +268,34 @@ def test_sample_bit_exact_many_blocks(dev, spread):
     assert np.array_equal(_sample_on(dev, n, amp, u), O.sample(amp, n, u))
 
 
+def test_sample_spans_with_zero_regions(dev):
+    """The chain composes spans of 4096 blocks: 25 qubits = 8192 blocks, with
+    the first 3/8 of the amplitudes zero (the running sum is 0: the subnormal
+    grid's fast path), a zero gap in the middle and magnitudes over many
+    binades elsewhere (spans that stop at a block leaving its binade and
+    restart after it), against the oracle's sampler.  The statistics show the
+    zero blocks composed in spans, not folded one by one."""
+    n = 25
+    rng = np.random.default_rng(2525)
+    size = 1 << n
+    mag = np.exp(-rng.uniform(0, 30, size))
+    mag[: 3 * size // 8] = 0.0
+    mag[size // 2: size // 2 + size // 16] = 0.0
+    amp = mag * np.exp(1j * rng.uniform(0, 2 * np.pi, size))
+    amp /= np.linalg.norm(amp)
+    st = StateVector(n, dev)
+    st.upload(amp)
+    u = boundary_uniforms(amp, n, 300, 25)
+    out = np.empty(len(u), dtype=np.uint64)
+    L.check(L.lib.qse_sample(st.handle, u.ctypes.data_as(L._pd), len(u), 0, out.ctypes.data_as(L._pu64)))
+    assert np.array_equal(out, O.sample(amp, n, u))
+    stats = (C.c_uint32 * 4)()
+    L.check(L.lib.qse_sampler_stats(st.handle, stats))
+    spans, single, exact, nb = list(stats)
+    assert nb == size // 4096
+    assert exact < 64 and single < 64, list(stats)
+
+
 @pytest.mark.parametrize("n", [5, 14, 18])
 def test_sample_after_execute(dev, n):
     # end to end: outcomes equal the oracle's sampler on the device state; against the

@@ -121,7 +121,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _worker(rank, world, port, outdir):
+def _worker(rank, world, port, outdir, chunk_bytes=256 << 20):
     import sys
     sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
     import datetime
@@ -139,7 +139,7 @@ def _worker(rank, world, port, outdir):
         shard = np.zeros(1 << nl, dtype=np.complex128)
         if rank == 0:
             shard[0] = 1.0
-        tr = S.TorchDistTransport(torch.from_numpy(shard), rank, dist)
+        tr = S.TorchDistTransport(torch.from_numpy(shard), rank, dist, chunk_bytes=chunk_bytes)
 
         def execute(local_ops):
             shard[:] = Ow.run_on(shard, nl, local_ops)
@@ -150,11 +150,26 @@ def _worker(rank, world, port, outdir):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 4])
-def test_gloo_ranks_exchange_halves(tmp_path, world):
+def test_exchange_pieces_cover_the_half_once():
+    for rows, cols, chunk in [(1, 512, 512), (1, 512, 100), (8, 64, 64), (8, 64, 200), (16, 4, 3), (4, 16, 1),
+                              (2, 1 << 20, 1 << 18)]:
+        seen = np.zeros((rows, cols), dtype=np.int32)
+        last = -1
+        for r0, nr, c0, nc in S.exchange_pieces(rows, cols, chunk):
+            assert 0 < nr * nc <= max(chunk, 1)
+            seen[r0:r0 + nr, c0:c0 + nc] += 1
+            assert r0 * cols + c0 > last      # address order
+            last = r0 * cols + c0
+        assert np.all(seen == 1), (rows, cols, chunk)
+
+
+# chunk sizes: one piece per exchange (256 MiB), and pieces of 4 and 3 amplitudes
+# (whole rows, cut rows, and ragged last pieces, each pipelined two deep)
+@pytest.mark.parametrize("world,chunk_bytes", [(2, 256 << 20), (4, 256 << 20), (2, 64), (4, 48)])
+def test_gloo_ranks_exchange_halves(tmp_path, world, chunk_bytes):
     ctx = mp.get_context("spawn")
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, str(tmp_path))) for r in range(world)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, str(tmp_path), chunk_bytes)) for r in range(world)]
     for p in procs:
         p.start()
     for p in procs:
