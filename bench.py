@@ -560,6 +560,13 @@ def main():
     for name, a, b in (("execute_ms", 4, 5), ("sample_ms", 5, 6), ("measure_ms", 6, 7)):
         L.check(lib.qse_ctx_elapsed(dev.handle, a, b, C.byref(ms)))
         phases[name] = ms.value
+    # the exact scan's path statistics on the executed state (untimed)
+    L.check(lib.qse_state_reset(st.handle))
+    L.check(lib.qse_execute(st.handle, L.dptr(ops), ngates, None, 0, None, None, 0, None))
+    sst = (C.c_uint32 * 4)()
+    L.check(lib.qse_sampler_stats(st.handle, sst))
+    phases["sampler_scan"] = {"spans": int(sst[0]), "single_blocks": int(sst[1]), "exact_blocks": int(sst[2]),
+                              "blocks": int(sst[3])}
 
     # HBM roofline of the pass kernel.  Each step resets the state, so the first
     # pass of every execute starts from |0..0> generated in registers and only

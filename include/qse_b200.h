@@ -267,9 +267,10 @@ QSE_API int qse_measure_qubit(qse_state* st, uint32_t qubit, double u, int32_t* 
  * outcome's amplitudes (renormalised) move to the qubit-0 half and the qubit is
  * left in |0>.  outcome and prob1 may be NULL. */
 QSE_API int qse_reset_qubit(qse_state* st, uint32_t qubit, double u, int32_t* outcome, double* prob1);
-/* Diagnostics of the exact-CDF scan on the current state: out = {chunks composed
- * in parallel, chunks walked block by block, blocks folded element by element,
- * blocks}.  Rebuilds the cumulative array. */
+/* Diagnostics of the exact cumulative scan on the current state: out = {spans
+ * of blocks composed in parallel, blocks handled on their own (no fold on the
+ * running sum's binade, or the sum leaves it inside the block), blocks folded
+ * element by element, blocks}.  Reruns the scan. */
 QSE_API int qse_sampler_stats(qse_state* st, uint32_t out[4]);
 /* total probability as the reference's sequential loop rounds it */
 QSE_API int qse_total_probability(qse_state* st, double* total);

@@ -631,8 +631,10 @@ __global__ void __launch_bounds__(kGT) k_guess_fin(const double* __restrict__ bs
     for (uint32_t w = 0; w < warp; ++w) wo += wsc[w];
     if (b >= nb) return;
     const double lo_c = o + wo + (inc - v), hi_c = o + wo + inc;
-    // conservative slack for the difference between this sum and the sequential one
-    const double slack = hi_c * 0x1.0p-20 + 1e-300;
+    // conservative slack for the difference between this sum and the sequential
+    // one (relative: sums of the same non-negative terms in another order; a
+    // zero sum is exact, so leading zero blocks get binade -1022)
+    const double slack = hi_c * 0x1.0p-20;
     const int e1 = lo_c - slack > 2.2250738585072014e-308 ? ilogb(lo_c - slack) : -1022;
     const int e2 = hi_c + slack > 2.2250738585072014e-308 ? ilogb(hi_c + slack) : -1022;
     // 2 e1 + 1 when the block may reach binade e1 + 1, 2 e1 when it stays in e1
@@ -672,7 +674,7 @@ constexpr int kWriteCTAs = 2;
 // above 2^53 stays there under rounding: the block then leaves the binade).
 // Only a binade with a tie composes the maps in element order, after the block
 // is restaged so that thread tid holds elements tid * kEPT .. + kEPT - 1.
-__device__ __forceinline__ Summ block_summ(const double (&p)[kEPT], int32_t gs, uint64_t* sh, double* stage)
+__device__ __forceinline__ Summ block_summ(double (&p)[kEPT], int32_t gs, uint64_t* sh, double* stage)
 {
     const int32_t e = gs >> 1;          // arithmetic shift: floor(gs / 2)
     const int nbin = 1 + (gs & 1);      // binades the block may run in
@@ -730,8 +732,7 @@ __device__ __forceinline__ Summ block_summ(const double (&p)[kEPT], int32_t gs, 
         all &= unsigned(sh[2 * (kBT / 32) + w]);
     }
     __syncthreads();   // sh is reused below
-    bool staged = false;
-    double q[kEPT];
+    bool staged = false;    // p restaged in element order (each binade's sums are already taken)
     for (int k = 0; k < nbin; ++k) {
         if (!((all >> (2 * k)) & 1)) continue;  // an element leaves binade e+k by itself: no fold there
         if ((all >> (2 * k + 1)) & 1) {
@@ -743,7 +744,7 @@ __device__ __forceinline__ Summ block_summ(const double (&p)[kEPT], int32_t gs, 
                 for (int j = 0; j < kEPT; ++j) stage[stage_slot(j * kBT + threadIdx.x)] = p[j];
                 __syncthreads();
 #pragma unroll
-                for (int j = 0; j < kEPT; ++j) q[j] = stage[threadIdx.x * kPad + j];
+                for (int j = 0; j < kEPT; ++j) p[j] = stage[threadIdx.x * kPad + j];
                 staged = true;
             }
             const Grid g = grid_of(e + k);
@@ -751,7 +752,7 @@ __device__ __forceinline__ Summ block_summ(const double (&p)[kEPT], int32_t gs, 
 #pragma unroll
             for (int j = 0; j < kEPT; ++j) {
                 uint64_t a0, a1, r0, r1;
-                elem_map_g(q[j], g, a0, a1);
+                elem_map_g(p[j], g, a0, a1);
                 compose(t0, t1, a0, a1, r0, r1);
                 t0 = r0;
                 t1 = r1;
@@ -769,8 +770,9 @@ __device__ __forceinline__ Summ block_summ(const double (&p)[kEPT], int32_t gs, 
 }
 
 // One CTA per block: the block's probabilities straight into registers
-// (coalesced, no staging unless a binade has a tie), then its fold.
-__global__ void __launch_bounds__(kBT) k_cdf_summ(const double* __restrict__ prob,
+// (coalesced, no staging unless a binade has a tie), then its fold.  Four
+// CTAs per SM (64 registers) keep 128 KiB of loads in flight per SM.
+__global__ void __launch_bounds__(kBT, 4) k_cdf_summ(const double* __restrict__ prob,
                                                   const int32_t* __restrict__ guess, Summ* __restrict__ summ)
 {
     __shared__ uint64_t sh[160];
@@ -788,24 +790,44 @@ __global__ void __launch_bounds__(kBT) k_cdf_summ(const double* __restrict__ pro
     if (threadIdx.x == blockDim.x - 1) summ[blockIdx.x] = out;
 }
 
-// blocks composed per thread in one step of the chain
-constexpr int kChainPer = 16;
+// blocks composed per thread in one step of the chain (9: a thread's records
+// start 45 8-byte words apart, so 16 threads hit 16 distinct bank pairs)
+constexpr int kChainPer = 9;
+constexpr uint32_t kSpan = uint32_t(kChainPer) * kBT;
+// dynamic shared memory of k_cdf_chain: two spans of fold records
+constexpr size_t kChainSmem = 2 * size_t(kSpan) * sizeof(Summ);
+static_assert(sizeof(Summ) % 8 == 0, "fold records are copied as 8-byte words");
+
+// The fold records summ[base, base + cnt) into shared memory by 8-byte
+// asynchronous copies, committed as one group.
+__device__ __forceinline__ void summ_prefetch(Summ* dst, const Summ* src, uint32_t base, uint32_t cnt)
+{
+    const uint64_t* s = reinterpret_cast<const uint64_t*>(src + base);
+    const uint32_t d = uint32_t(__cvta_generic_to_shared(dst));
+    const uint32_t words = cnt * uint32_t(sizeof(Summ) / 8);
+    for (uint32_t i = threadIdx.x; i < words; i += kBT)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d + 8 * i), "l"(s + i) : "memory");
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
 
 // Single CTA: the exact running sum block by block.  cin[b] = exact sum
 // before block b; cin[nb] = total.  A running sum of zero is on the grid of
 // binade -1022 (spacing 2^-1074, shared by the subnormals), where zero and
-// subnormal blocks fold exactly, so leading zero blocks take the fast path.  Each step takes the next span of up to
-// kChainPer * kBT blocks (kChainPer consecutive per thread): every block up to
-// the first one without a fold on the running sum's binade composes with one
-// block-wide scan, and the step commits the blocks up to the first one whose
-// sum would leave the binade (or the one without a fold).  That block is
-// handled on its own (its fold on the binade it actually starts in, else an
-// exact element-by-element fold) and the next span starts after it, so every
-// step advances past every block it could commit.
-__global__ void __launch_bounds__(kBT) k_cdf_chain(const double* __restrict__ prob,
+// subnormal blocks fold exactly, so leading zero blocks take the fast path.
+// Each step takes the next span of up to kSpan blocks (kChainPer consecutive
+// per thread): every block up to the first one without a fold on the running
+// sum's binade composes with one block-wide scan, and the step commits the
+// blocks up to the first one whose sum would leave the binade (or the one
+// without a fold).  That block is handled on its own (its fold on the binade
+// it actually starts in, else an exact element-by-element fold) and the next
+// span starts after it.  The fold records of a span arrive in shared memory
+// while the previous span is composed (two buffers; a span that stopped early
+// reloads its successor's records).
+__global__ void __launch_bounds__(kBT, 1) k_cdf_chain(const double* __restrict__ prob,
                                                    const Summ* __restrict__ summ, uint32_t nb, double* __restrict__ cin,
                                                    uint32_t* __restrict__ stats)
 {
+    extern __shared__ Summ sbuf[];
     __shared__ uint64_t sh[160];
     __shared__ double stage[kBT * kPad];
     __shared__ double s_c;
@@ -814,12 +836,28 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double* __restrict__ pr
     uint32_t n_span = 0, n_single = 0, n_exact = 0;  // statistics (thread 0)
     const uint32_t t = threadIdx.x;
     if (t == 0) s_c = 0.0;
+    uint32_t base = 0, loaded = 0, cur = 0;   // buffer cur holds the records from `loaded` on
+    summ_prefetch(sbuf, summ, 0, min(kSpan, nb));
     __syncthreads();
-    uint32_t base = 0;
     while (base < nb) {
+        const uint32_t span = min(kSpan, nb - base);
+        if (loaded != base) {   // the previous span stopped early: its successor's records
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+            __syncthreads();
+            summ_prefetch(sbuf + cur * kSpan, summ, base, span);
+            loaded = base;
+        }
+        const uint32_t next = base + span;
+        if (next < nb) {
+            summ_prefetch(sbuf + (cur ^ 1) * kSpan, summ, next, min(kSpan, nb - next));
+            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        } else {
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        }
+        __syncthreads();
+        const Summ* rec = sbuf + cur * kSpan;
         const double c = s_c;
         const int e0 = epoch_of(c);
-        const uint32_t span = min(uint32_t(kChainPer * kBT), nb - base);
         const uint32_t p0 = t * kChainPer;           // this thread's first position in the span
         uint64_t d0[kChainPer], d1[kChainPer];
         uint32_t my_bad = span;
@@ -827,8 +865,7 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double* __restrict__ pr
         for (int k = 0; k < kChainPer; ++k) {
             d0[k] = d1[k] = 0;
             const uint32_t pos = p0 + k;
-            if (pos < span && !summ_pick(summ[base + pos], e0, d0[k], d1[k]) && my_bad == span)
-                my_bad = pos;
+            if (pos < span && !summ_pick(rec[pos], e0, d0[k], d1[k]) && my_bad == span) my_bad = pos;
         }
         if (t == 0) s_end = span;
         __syncthreads();
@@ -838,7 +875,7 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double* __restrict__ pr
         uint64_t m0 = 0, m1 = 0;
 #pragma unroll
         for (int k = 0; k < kChainPer; ++k) {
-            if (p0 + k >= bad) d0[k] = d1[k] = 0;     // identity beyond the first block without a fold
+            if (p0 + k >= bad) d0[k] = d1[k] = 0;     // identity from the first block without a fold on
             uint64_t r0, r1;
             compose(m0, m1, d0[k], d1[k], r0, r1);
             m0 = r0;
@@ -873,9 +910,11 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double* __restrict__ pr
             if (pos + 1 == end) s_c = ldexp(double(xin[k] + ((xin[k] & 1) ? d1[k] : d0[k])), e0 - 52);
         }
         if (t == 0 && end > 0) ++n_span;
-        __syncthreads();
+        __syncthreads();   // every thread is done with rec and s_c before either changes
         if (end >= span) {
-            base += span;
+            base = next;
+            loaded = next;
+            cur ^= 1;
             continue;
         }
         // block b starts in the running sum's binade but has no fold there or leaves it
@@ -887,7 +926,7 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double* __restrict__ pr
             const int eb = epoch_of(cc);
             uint64_t b0, b1;
             int slow = 1;
-            if (summ_pick(summ[b], eb, b0, b1)) {
+            if (summ_pick(rec[end], eb, b0, b1)) {
                 uint64_t Cb = cc > 0.0 ? uint64_t(ldexp(cc, 52 - eb)) : 0;
                 uint64_t Co = Cb + ((Cb & 1) ? b1 : b0);
                 if (Co < kTwo53 && Co >= Cb) {
@@ -908,6 +947,7 @@ __global__ void __launch_bounds__(kBT) k_cdf_chain(const double* __restrict__ pr
         __syncthreads();
         base = b + 1;
     }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     if (t == 0) {
         cin[nb] = s_c;
         if (stats) {
@@ -1335,7 +1375,9 @@ CdfView build_cdf(qse_state* st)
         k_guess_part<<<ng, kGT, 0, ctx->stream>>>(bsum, nb, gtot);
         k_guess_fin<<<ng, kGT, 0, ctx->stream>>>(bsum, nb, gtot, guess);
         k_cdf_summ<<<nb, kBT, 0, ctx->stream>>>(v.cdf, guess, summ);
-        k_cdf_chain<<<1, kBT, 0, ctx->stream>>>(v.cdf, summ, nb, v.cin, reinterpret_cast<uint32_t*>(v.cin + nb + 1));
+        QSE_CUDA(cudaFuncSetAttribute(k_cdf_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kChainSmem)));
+        k_cdf_chain<<<1, kBT, kChainSmem, ctx->stream>>>(v.cdf, summ, nb, v.cin,
+                                                        reinterpret_cast<uint32_t*>(v.cin + nb + 1));
         QSE_CUDA(cudaGetLastError());
         count_launch(ctx, 4);
         // the array keeps the probabilities: shots rebuild the cumulative values
@@ -1463,8 +1505,8 @@ double total_probability(qse_state* st)
 }  // namespace qse
 
 namespace qse {
-// chain statistics of the last exact-CDF build of st: fast chunks, slow
-// chunks, blocks folded exactly, blocks (zeros for states below one block)
+// chain statistics of the last exact scan of st: spans, single blocks,
+// blocks folded exactly, blocks (zeros for states below one block)
 void sampler_stats(qse_state* st, uint32_t out[4])
 {
     st->cdf_version = ~uint64_t(0);
