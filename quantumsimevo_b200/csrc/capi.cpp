@@ -170,6 +170,7 @@ int qse_ctx_destroy(qse_ctx* ctx)
     if (!ctx) return QSE_OK;
     bind_device(ctx);
     cudaStreamSynchronize(ctx->stream);
+    qse::destroy_compact_state(ctx);
     ctx->plan_buf.release();
     ctx->scratch.release();
     ctx->scratch2.release();

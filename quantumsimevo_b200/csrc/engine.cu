@@ -252,9 +252,11 @@ plan::Plan plan_for(qse_state* st, const std::vector<plan::Gate>& gates, plan::O
     srcs.clear();
     if (!use_jit) return pl;
     srcs.reserve(pl.passes.size());
-    for (size_t i = 0; i < pl.passes.size(); ++i)
-        srcs.push_back(jit::generate(pl.passes[i], ns, i == 0 && ns == 1 && st->lazy_basis, st->ctx->jit == 2,
-                                     st->n >= jit::kPreGroupQubits));
+    for (size_t i = 0; i < pl.passes.size(); ++i) {
+        const bool basis_in = i == 0 && ns == 1 && st->lazy_basis;
+        srcs.push_back(jit::generate(pl.passes[i], ns, basis_in, st->ctx->jit == 2, st->n >= jit::kPreGroupQubits,
+                                     basis_in ? st->lazy_umask : 0));
+    }
     if (st->n >= kJitAlwaysQubits || jit::count_uncached(srcs) <= kJitMaxNewKernels) return pl;
     use_jit = false;
     srcs.clear();
@@ -288,6 +290,9 @@ struct PassRunner {
 
     void run(size_t i, double2* lam, double* part)
     {
+        // the first pass of a compact-input plan reads the compact state
+        if (jit && i == 0 && ns == 1 && st->lazy_basis && st->lazy_umask)
+            lam = const_cast<double2*>(static_cast<const double2*>(st->lazy_src));
         tile::PassArgs a = up.args[i];
         a.psi = reinterpret_cast<double2*>(st->amp);
         a.lam = lam;
@@ -370,7 +375,175 @@ void run_noise(qse_state* st, qse_noise* nz, const qse_op* ops, size_t nops, con
     QSE_CUDA(cudaStreamSynchronize(ctx->stream));
 }
 
+plan::Options fused_options(const qse_ctx* ctx, uint32_t n)
+{
+    plan::Options opt;
+    opt.rb = 4;
+    opt.k = tile_qubits_for(ctx, n, 4, 12);
+    opt.max_gates = uint32_t(std::max(0, ctx->max_gates_per_pass));
+    if (ctx->jit && (opt.max_gates == 0 || opt.max_gates > plan::kJitMaxGates)) opt.max_gates = plan::kJitMaxGates;
+    opt.zz_fuse = true;
+    return opt;
+}
+
+// Forward passes of gates on st through the planner; returns the pass count.
+uint64_t run_fused(qse_state* st, const std::vector<plan::Gate>& gates)
+{
+    qse_ctx* ctx = st->ctx;
+    bool use_jit = false;
+    std::vector<jit::Source> srcs;
+    plan::Plan pl = plan_for(st, gates, fused_options(ctx, st->n), 1, use_jit, srcs);
+    if (!use_jit) materialize(st);  // interpreter passes read the state
+    Uploaded up = upload_plan(ctx, pl, use_jit && st->n >= jit::kPreGroupQubits);
+    PassRunner runner(st, pl, up, 1, 4, use_jit, std::move(srcs));
+    for (size_t i = 0; i < up.args.size(); ++i) runner.run(i, nullptr, nullptr);
+    if (!up.args.empty()) {   // the first pass wrote every amplitude
+        st->lazy_basis = false;
+        st->lazy_umask = 0;
+        st->lazy_src = nullptr;
+    }
+    for (uint32_t q = 0; q < st->n; ++q) st->perm[q] = pl.perm_final[q];
+    return pl.passes.size();
+}
+
+// ---- compact prefix ----
+// A circuit started from a basis state touches its qubits progressively (a
+// QFT's first passes act on its low qubits while the others are still |0>).
+// While the qubits touched so far are few, the state is that of those qubits
+// times the untouched qubits' basis bits, so the leading passes can run on a
+// state of only the touched qubits: 2^m amplitudes (at most 64 MiB, resident
+// in L2) instead of 2^n.  The first pass over the full state then reads its
+// input from that compact state (jit.cpp, compact input) instead of from HBM.
+// Untouched here means untouched by any gate, diagonal ones included, so the
+// compact circuit is the prefix's gates unchanged with its qubits renumbered.
+constexpr uint32_t kCompactMinQubits = 24;   // full states this large (smaller ones gain little)
+constexpr uint32_t kCompactMaxQubits = 22;   // compact states up to this size
+
+uint64_t gate_qubits(const plan::Gate& g)
+{
+    auto b = [](uint32_t q) { return uint64_t(1) << q; };
+    switch (g.type) {
+    case QSE_GATE_IDENTITY: return 0;
+    case QSE_GATE_CNOT: case QSE_GATE_CPHASE: case QSE_GATE_SWAP: return b(g.t) | b(g.c);
+    case QSE_GATE_MCPHASE: return b(g.t) | g.cmask;
+    default: return b(g.t);
+    }
+}
+
+qse_state* compact_state(qse_ctx* ctx, uint32_t m)
+{
+    if (!ctx->compact) {
+        auto* cs = new qse_state;
+        cs->ctx = ctx;
+        cs->n = kCompactMaxQubits;
+        if (cudaMalloc(&cs->amp, cs->size() * 16) != cudaSuccess) {
+            cudaGetLastError();
+            delete cs;
+            fail(QSE_ERR_OOM, "device allocation of the compact state failed");
+        }
+        ctx->compact = cs;
+    }
+    qse_state* cs = ctx->compact;
+    cs->n = m;
+    for (uint32_t q = 0; q < 64; ++q) cs->perm[q] = q;
+    cs->touch();
+    return cs;
+}
+
+// Runs the longest prefix of the plan's passes (at least two) whose gates
+// touch at most kCompactMaxQubits qubits on the compact state and leaves st
+// in the lazy compact form; rest = the other gates in program order (a valid
+// order: every gate of the prefix passes runs before every other gate in the
+// plan).  False (nothing done) when no such prefix exists.
+bool compact_prefix(qse_state* st, const std::vector<plan::Gate>& gates_in, std::vector<plan::Gate>& rest,
+                    uint64_t& passes)
+{
+    qse_ctx* ctx = st->ctx;
+    if (!ctx->jit || !st->lazy_basis || st->lazy_umask || st->n < kCompactMinQubits) return false;
+    // the zz rewrite moves gates between slots: apply it first so that the
+    // plan's source indices name the gates that run
+    plan::Options opt = fused_options(ctx, st->n);
+    std::vector<plan::Gate> fused;
+    const std::vector<plan::Gate>& gates = plan::fuse_zz(gates_in, fused) ? fused : gates_in;
+    opt.zz_fuse = false;
+    opt.acc_mul = true;
+    const plan::Plan pl = plan::build(gates, st->n, st->perm, opt);
+    size_t K = 0;
+    uint64_t u = 0, uK = 0;
+    for (size_t i = 0; i < pl.passes.size(); ++i) {
+        for (uint32_t g : pl.passes[i].order) u |= gate_qubits(gates[g]);
+        if (uint32_t(__builtin_popcountll(u)) > kCompactMaxQubits) break;
+        K = i + 1;
+        uK = u;
+    }
+    if (K < 2) return false;
+    // compact qubit r = the touched qubit with the r-th lowest physical position
+    std::vector<uint32_t> qs;
+    for (uint32_t q = 0; q < st->n; ++q)
+        if ((uK >> q) & 1) qs.push_back(q);
+    std::sort(qs.begin(), qs.end(), [&](uint32_t a, uint32_t b) { return st->perm[a] < st->perm[b]; });
+    const uint32_t m = uint32_t(qs.size());
+    uint32_t rank[64] = {0};
+    uint64_t umask = 0, cbasis = 0;
+    for (uint32_t r = 0; r < m; ++r) {
+        rank[qs[r]] = r;
+        umask |= uint64_t(1) << st->perm[qs[r]];
+        cbasis |= ((st->lazy_index >> st->perm[qs[r]]) & 1) << r;
+    }
+    std::vector<char> in_prefix(gates.size(), 0);
+    std::vector<plan::Gate> sub;
+    for (size_t i = 0; i < K; ++i)
+        for (uint32_t g : pl.passes[i].order) {
+            in_prefix[g] = 1;
+            plan::Gate x = gates[g];
+            x.t = rank[x.t];
+            if (x.type == QSE_GATE_CNOT || x.type == QSE_GATE_CPHASE || x.type == QSE_GATE_SWAP) x.c = rank[x.c];
+            if (x.type == QSE_GATE_MCPHASE) {
+                uint64_t cm = 0;
+                for (uint64_t b = x.cmask; b; b &= b - 1) cm |= uint64_t(1) << rank[__builtin_ctzll(b)];
+                x.cmask = cm;
+            }
+            sub.push_back(x);
+        }
+    rest.clear();
+    for (size_t g = 0; g < gates.size(); ++g)
+        if (!in_prefix[g]) rest.push_back(gates[g]);
+    // the prefix on the compact state (its passes are not the full state's:
+    // they stay out of the pass timings)
+    qse_state* cs = compact_state(ctx, m);
+    mark_basis(cs, cbasis);
+    const bool timing = ctx->time_passes;
+    ctx->time_passes = false;
+    try {
+        if (m < 4) {   // as execute_program runs states this small: gate by gate
+            materialize(cs);
+            for (const plan::Gate& g : sub) apply_plain(cs, g);
+            passes = sub.size();
+        } else {
+            passes = run_fused(cs, sub);
+        }
+        materialize(cs);
+        canonicalize(cs);
+    } catch (...) {
+        ctx->time_passes = timing;
+        throw;
+    }
+    ctx->time_passes = timing;
+    st->lazy_umask = umask;
+    st->lazy_src = cs->amp;
+    return true;
+}
+
 }  // namespace
+
+void destroy_compact_state(qse_ctx* ctx)
+{
+    if (!ctx->compact) return;
+    cudaFree(ctx->compact->amp);
+    if (ctx->compact->aux) cudaFree(ctx->compact->aux);
+    delete ctx->compact;
+    ctx->compact = nullptr;
+}
 
 void execute_program(qse_state* st, const qse_op* ops, size_t nops, const double* params, size_t nparams,
                      qse_noise* noise, const double* inj, size_t ninj, qse_exec_stats* stats)
@@ -395,22 +568,14 @@ void execute_program(qse_state* st, const qse_op* ops, size_t nops, const double
         for (const plan::Gate& g : gates) apply_plain(st, g);
         passes = gates.size();
     } else {
-        plan::Options opt;
-        opt.rb = 4;
-        opt.k = tile_qubits_for(ctx, st->n, 4, 12);
-        opt.max_gates = uint32_t(std::max(0, ctx->max_gates_per_pass));
-        if (ctx->jit && (opt.max_gates == 0 || opt.max_gates > plan::kJitMaxGates)) opt.max_gates = plan::kJitMaxGates;
-        opt.zz_fuse = true;
-        bool use_jit = false;
-        std::vector<jit::Source> srcs;
-        plan::Plan pl = plan_for(st, gates, opt, 1, use_jit, srcs);
-        if (!use_jit) materialize(st);  // interpreter passes read the state
-        Uploaded up = upload_plan(ctx, pl, use_jit && st->n >= jit::kPreGroupQubits);
-        PassRunner runner(st, pl, up, 1, 4, use_jit, std::move(srcs));
-        for (size_t i = 0; i < up.args.size(); ++i) runner.run(i, nullptr, nullptr);
-        if (!up.args.empty()) st->lazy_basis = false;  // the first pass wrote every amplitude
-        for (uint32_t q = 0; q < st->n; ++q) st->perm[q] = pl.perm_final[q];
-        passes = pl.passes.size();
+        std::vector<plan::Gate> rest;
+        uint64_t compact_passes = 0;
+        if (compact_prefix(st, gates, rest, compact_passes)) {
+            passes = compact_passes + run_fused(st, rest);
+            materialize(st);   // no pass consumed the compact form (nothing after the prefix)
+        } else {
+            passes = run_fused(st, gates);
+        }
     }
     if (noise && noise->cfg.enabled) launch_pauli_frame(st, noise->d_counts);
     if (stats) {

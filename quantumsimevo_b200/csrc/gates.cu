@@ -439,6 +439,8 @@ void mark_basis(qse_state* st, uint64_t phys_index)
 {
     st->lazy_basis = true;
     st->lazy_index = phys_index;
+    st->lazy_umask = 0;
+    st->lazy_src = nullptr;
     st->touch();
 }
 
@@ -446,9 +448,42 @@ namespace {
 void write_basis_state(qse_state* st, uint64_t phys_index)
 {
     st->lazy_basis = false;
+    st->lazy_umask = 0;
+    st->lazy_src = nullptr;
     st->touch();
     QSE_CUDA(cudaMemsetAsync(st->amp, 0, st->size() * 16, st->ctx->stream));
     k_set_one<<<1, 1, 0, st->ctx->stream>>>(reinterpret_cast<double2*>(st->amp), phys_index);
+    QSE_CUDA(cudaGetLastError());
+    count_launch(st->ctx);
+}
+
+// out[pdep(i, umask) | fixed] = src[i] for i < count (count = 2^popcount(umask);
+// every other amplitude was zeroed before)
+__global__ void __launch_bounds__(kBlock) k_expand_compact(double2* __restrict__ out, const double2* __restrict__ src,
+                                                          uint64_t count, uint64_t umask, uint64_t fixed)
+{
+    for (uint64_t i = blockIdx.x * uint64_t(kBlock) + threadIdx.x; i < count; i += uint64_t(gridDim.x) * kBlock) {
+        uint64_t x = fixed, r = i;
+        for (uint64_t m = umask; m; m &= m - 1, r >>= 1)
+            if (r & 1) x |= m & (~m + 1);
+        out[x] = src[i];
+    }
+}
+
+// the compact form of a lazy state written out: zeros, then the compact
+// amplitudes at their places
+void write_compact_state(qse_state* st)
+{
+    const uint64_t umask = st->lazy_umask, fixed = st->lazy_index & ~umask;
+    const double2* src = static_cast<const double2*>(st->lazy_src);
+    st->lazy_basis = false;
+    st->lazy_umask = 0;
+    st->lazy_src = nullptr;
+    st->touch();
+    QSE_CUDA(cudaMemsetAsync(st->amp, 0, st->size() * 16, st->ctx->stream));
+    const uint64_t count = uint64_t(1) << __builtin_popcountll(umask);
+    k_expand_compact<<<grid_full(count), kBlock, 0, st->ctx->stream>>>(reinterpret_cast<double2*>(st->amp), src, count,
+                                                                       umask, fixed);
     QSE_CUDA(cudaGetLastError());
     count_launch(st->ctx);
 }
@@ -456,7 +491,9 @@ void write_basis_state(qse_state* st, uint64_t phys_index)
 
 void materialize(qse_state* st)
 {
-    if (st->lazy_basis) write_basis_state(st, st->lazy_index);
+    if (!st->lazy_basis) return;
+    if (st->lazy_umask) write_compact_state(st);
+    else write_basis_state(st, st->lazy_index);
 }
 
 // StateVector::measureQubit / resetQubit (StateVector.cpp:158-221) with the

@@ -96,6 +96,10 @@ struct Gen {
 
     bool zero_in = false;   // generate the basis state |bi> instead of loading (ns == 1)
     int basis_slot = -1;    // prm slot of bi (set per launch)
+    // with zero_in: physical qubits whose input comes from a compact state
+    // (lam, 2^popcount(umask) amplitudes indexed by those bits in ascending
+    // order); the other qubits hold the bits of bi.  0: the plain basis state
+    uint64_t umask = 0;
     bool xb_used = false;   // the exchange buffer holds data some thread may still read
     std::string SYNC = "__syncthreads();";   // barrier of the threads that share xb
     // gradient slots accumulated per thread (slot -> accumulator index)
@@ -106,9 +110,10 @@ struct Gen {
     // and calling sincos per group
     bool pre_gv = false;
 
-    Gen(const plan::PassProgram& p, int nstates, bool zero_input, bool precomputed_groups = false)
-        : P(p), ns(nstates), zero_in(zero_input && nstates == 1),
-          pre_gv(precomputed_groups && !(zero_input && nstates == 1) && !p.groups.empty())
+    Gen(const plan::PassProgram& p, int nstates, bool zero_input, bool precomputed_groups = false,
+        uint64_t compact_mask = 0)
+        : P(p), ns(nstates), zero_in(zero_input && nstates == 1), umask(zero_in ? compact_mask : 0),
+          pre_gv(precomputed_groups && (!zero_in || umask != 0) && !p.groups.empty())
     {
         R = 1u << P.rb;
         T = 1u << (P.k - P.rb);
@@ -438,22 +443,27 @@ struct Gen {
             // one kernel serves every index): only the tile holding bi has a nonzero
             // amplitude; every gate is linear, so every other tile's output is zero,
             // stored in tile-local order m = tid + j*T (the tile always holds physical
-            // qubits 0..2, so consecutive threads write consecutive amplitudes)
+            // qubits 0..2, so consecutive threads write consecutive amplitudes).
+            // Compact input (umask): the input is zero unless the bits outside umask
+            // equal bi's, so a tile whose outer bits outside umask differ stores zeros
             basis_slot = int(push(0.0));
-            o << "  const u64 bi = (u64)P.v[" << basis_slot << "];\n";
+            o << "  const u64 bi = (u64)P.v[" << basis_slot << "]; (void)bi;\n";
             const uint32_t lt = uint32_t(__builtin_ctz(T));
-            o << "  if (ob != (bi & " << hex(P.outer_mask) << ")) {\n    const u64 gz = ob";
-            for (uint32_t b = 0; b < lt; ++b)
-                o << " | ((u64)((tid >> " << b << ") & 1u) << " << int(P.tile_phys[b]) << ")";
-            o << ";\n";
-            for (uint32_t j = 0; j < R; ++j) {
-                uint64_t cj = 0;
-                const uint64_t m = uint64_t(j) * T;
-                for (uint32_t b = lt; b < P.k; ++b)
-                    if ((m >> b) & 1) cj |= uint64_t(1) << P.tile_phys[b];
-                o << "    psi[gz + " << hex(cj) << "] = make_double2(0.0, 0.0);\n";
+            const uint64_t zmask = P.outer_mask & ~umask;
+            if (zmask) {
+                o << "  if (((ob ^ bi) & " << hex(zmask) << ") != 0ull) {\n    const u64 gz = ob";
+                for (uint32_t b = 0; b < lt; ++b)
+                    o << " | ((u64)((tid >> " << b << ") & 1u) << " << int(P.tile_phys[b]) << ")";
+                o << ";\n";
+                for (uint32_t j = 0; j < R; ++j) {
+                    uint64_t cj = 0;
+                    const uint64_t m = uint64_t(j) * T;
+                    for (uint32_t b = lt; b < P.k; ++b)
+                        if ((m >> b) & 1) cj |= uint64_t(1) << P.tile_phys[b];
+                    o << "    psi[gz + " << hex(cj) << "] = make_double2(0.0, 0.0);\n";
+                }
+                o << "    return;\n  }\n";
             }
-            o << "    return;\n  }\n";
         }
         // load first (gb holds only thread and outer bits, the offsets only
         // register bits: gb + off == gb | off, and the constant folds into the
@@ -465,6 +475,38 @@ struct Gen {
                 o << "  a0[" << j << "] = psi[gb + " << hex(reg_off(j)) << "];";
                 if (ns == 2) o << " a1[" << j << "] = lam[gb + " << hex(reg_off(j)) << "];";
                 o << "\n";
+            }
+        } else if (umask) {
+            // compact input: amplitude x = lam[pext(x, umask)] where x's other tile
+            // bits equal bi's, else 0 (pext of gb and of each register offset add:
+            // their bits are disjoint)
+            auto rank = [&](uint32_t q) { return __builtin_popcountll(umask & ((uint64_t(1) << q) - 1)); };
+            o << "  u64 cb = 0;\n  { u64 c = blockIdx.x;";
+            for (uint32_t q = 0; q < 64; ++q)
+                if ((P.outer_mask >> q) & 1) {
+                    if ((umask >> q) & 1) o << " cb |= (c & 1ull) << " << rank(q) << ";";
+                    o << " c >>= 1;";
+                }
+            o << " (void)c; }\n";
+            for (int t = 0; t < nthr; ++t) {
+                const uint32_t q = P.tile_phys[thr[t]];
+                if ((umask >> q) & 1) o << "  cb |= (u64)((tid >> " << t << ") & 1u) << " << rank(q) << ";\n";
+            }
+            uint64_t tmask = 0;
+            for (uint32_t b = 0; b < P.k; ++b) tmask |= uint64_t(1) << P.tile_phys[b];
+            const uint64_t tz = tmask & ~umask;
+            for (uint32_t j = 0; j < R; ++j) {
+                uint64_t coff = 0;
+                for (uint32_t i = 0; i < P.rb; ++i)
+                    if ((j >> i) & 1) {
+                        const uint32_t q = P.tile_phys[reg[i]];
+                        if ((umask >> q) & 1) coff |= uint64_t(1) << rank(q);
+                    }
+                o << "  a0[" << j << "] = ";
+                if (tz) o << "((((gb | " << hex(reg_off(j)) << ") ^ bi) & " << hex(tz) << ") == 0ull) ? ";
+                o << "lam[cb + " << hex(coff) << "]";
+                if (tz) o << " : make_double2(0.0, 0.0)";
+                o << ";\n";
             }
         }
         // prologue: per-CTA diagonal group values, then the lane tables
@@ -490,7 +532,7 @@ struct Gen {
         if (ntab) o << "  __syncthreads();\n" << tabs.str();
         if (ns == 2 && nslots) o << "  for (u32 i = tid; i < " << nslots * NW << "u; i += " << T << "u) wp[i] = 0.0;\n";
         o << "  __syncthreads();\n";
-        if (zero_in)
+        if (zero_in && !umask)
             for (uint32_t j = 0; j < R; ++j)
                 o << "  a0[" << j << "] = make_double2((gb | " << hex(reg_off(j)) << ") == bi ? 1.0 : 0.0, 0.0);\n";
         std::swap(o, head);
@@ -834,7 +876,8 @@ static bool streamable(const plan::PassProgram& p, int nstates, bool basis_input
            __builtin_popcountll(p.outer_mask) >= 10;
 }
 
-Source generate(const plan::PassProgram& p, int nstates, bool basis_input, bool streamed, bool precomputed_groups)
+Source generate(const plan::PassProgram& p, int nstates, bool basis_input, bool streamed, bool precomputed_groups,
+                uint64_t compact_mask)
 {
     if (streamed && streamable(p, nstates, basis_input)) {
         Gen g(p, nstates, false);
@@ -848,7 +891,7 @@ Source generate(const plan::PassProgram& p, int nstates, bool basis_input, bool 
             return s;
         }
     }
-    Gen g(p, nstates, basis_input, precomputed_groups);
+    Gen g(p, nstates, basis_input, precomputed_groups, compact_mask);
     Source s;
     s.code = g.run();
     s.prm = std::move(g.prm);

@@ -51,9 +51,13 @@ size_t compile_only(const Source& s);
 // least 8 contiguous amplitudes); otherwise one CTA per tile
 // precomputed_groups: the pass reads its per-CTA diagonal group values from a
 // table computed beforehand (k_group_values: one row of ngroups values per
-// tile) instead of computing them in a prologue; not for basis-input passes
+// tile) instead of computing them in a prologue; not for plain basis-input
+// passes (their tiles but one store zeros)
+// compact_mask (with basis_input): the input is a compact state on the
+// physical qubits of the mask (passed as `lam` at launch, indexed by those
+// bits in ascending order) times the basis bits of i on the other qubits
 Source generate(const plan::PassProgram& p, int nstates, bool basis_input = false, bool streamed = false,
-                bool precomputed_groups = false);
+                bool precomputed_groups = false, uint64_t compact_mask = 0);
 // distinct sources among srcs that are not compiled yet
 size_t count_uncached(const std::vector<Source>& srcs);
 // compiled kernels for every source (cached by source text; missing ones are compiled in parallel)

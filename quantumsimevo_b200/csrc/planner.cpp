@@ -566,7 +566,7 @@ private:
 // c XOR t = c + t - 2ct: the diagonal RZ(th,c) PHASE(th,t) CPHASE(-2th,c,t), global
 // phase included.  QAOA cost layers written with CNOTs (QSEplayground/QAOA.cpp:128-133)
 // then need no pass of their own.  Returns false when nothing matched.
-static bool fuse_zz(const std::vector<Gate>& gates, std::vector<Gate>& out)
+bool fuse_zz(const std::vector<Gate>& gates, std::vector<Gate>& out)
 {
     bool any = false;
     for (size_t i = 0; i + 2 < gates.size(); ++i) {

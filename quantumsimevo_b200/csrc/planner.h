@@ -153,6 +153,12 @@ struct Plan {
     uint64_t gates = 0;
 };
 
+// The rewrite of Options::zz_fuse on its own: out = gates with every
+// CNOT(c,t) RZ(th,t) CNOT(c,t) (no gradient ids) replaced by RZ(th,c)
+// PHASE(th,t) CPHASE(-2th,c,t) in the same three slots; false (out untouched)
+// when there is none.
+bool fuse_zz(const std::vector<Gate>& gates, std::vector<Gate>& out);
+
 // Plans gates (logical qubits) for an n-qubit state whose logical->physical
 // map is perm_in.  Throws qse::Error on invalid gates.
 Plan build(const std::vector<Gate>& gates, uint32_t n, const uint32_t* perm_in, const Options& opt);

@@ -77,6 +77,10 @@ struct qse_ctx {
     bool time_passes = false;
     std::vector<cudaEvent_t> pass_events;  // pool, pairs (start, stop)
     size_t pass_events_used = 0;
+    // state of at most kCompactMaxQubits qubits on which an execute runs the
+    // leading passes of a circuit that leave the other qubits in their basis
+    // state (engine.cu, compact_prefix); allocated on first use
+    qse_state* compact = nullptr;
 };
 
 struct qse_state {
@@ -90,6 +94,11 @@ struct qse_state {
     uint64_t lazy_index = 0;     // but the array has not been written: the next fused execute
                                  // generates it in its first pass, every other reader calls
                                  // materialize() first (reset: |0..0>; measure: the outcome)
+    // with lazy_basis, inside one execute: the state is a compact state on the
+    // physical qubits of lazy_umask (lazy_src, indexed by those bits in
+    // ascending order) times the basis bits of lazy_index on the other qubits
+    uint64_t lazy_umask = 0;
+    const void* lazy_src = nullptr;
     // exact cumulative probabilities (sample.cu), valid while cdf_version == version
     qse::DevBuf cdf;
     uint64_t cdf_version = ~uint64_t(0);
@@ -153,7 +162,8 @@ void mark_basis(qse_state* st, uint64_t phys_index);                 // lazy |ph
 void mark_zero(qse_state* st);       // reset without writing: lazy |0..0>
 // StateVector::measureQubit (reset = false) / resetQubit (reset = true), draw u injected
 int measure_or_reset_qubit(qse_state* st, uint32_t qubit, double u, bool reset, double* prob1);
-void materialize(qse_state* st);     // write a lazy basis state into the array (no-op otherwise)
+void materialize(qse_state* st);     // write a lazy basis (or compact) state into the array (no-op otherwise)
+void destroy_compact_state(qse_ctx* ctx);
 void launch_pauli_frame(qse_state* st, const int32_t* d_counts);      // Noise::applyPauliNoise
 void permute_to_logical(qse_state* st, double* dst_device);           // gather into logical order
 void scale_state(qse_state* st, double s);
