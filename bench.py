@@ -573,20 +573,33 @@ def main():
     # writes (16 B per amplitude); the others read and write (32 B per
     # amplitude).  The roofline is taken on the read+write launches; the
     # execute's algorithmic bytes count both kinds.
+    # The pass timings list the passes over the full state only (passes that
+    # run on a compact state of the first touched qubits are not timed).  Every
+    # step resets, so the first full-state pass of an execute reads no full
+    # state: it generates its input (from |0..0>, or from the compact state of
+    # at most 2^22 amplitudes, under 0.5 % of its bytes at 30 qubits) and writes
+    # 16 B per amplitude; any later one reads and writes 32 B per amplitude.
     hbm_peak, peak_kind = peaks()
-    bytes_per_pass = 32.0 * (1 << n)
     ppe = max(1, int(round(passes_per_exec)))
     idx = np.arange(len(plist))
-    rw = plist[(idx % ppe) != 0] if ppe > 1 else plist
-    zs = plist[(idx % ppe) == 0] if ppe > 1 else plist[:0]
-    avg_pass_ms = float(rw.mean()) if rw.size else float(plist.mean())
+    rw = plist[(idx % ppe) != 0]
+    zs = plist[(idx % ppe) == 0]
+    if rw.size:
+        bytes_per_pass, avg_pass_ms = 32.0 * (1 << n), float(rw.mean())
+        kernel = "qse_pass"
+        launches_desc = "read+write full-state passes (all but the first of each execute)"
+    else:
+        bytes_per_pass, avg_pass_ms = 16.0 * (1 << n), float(zs.mean())
+        kernel = "qse_pass_compact_in"
+        launches_desc = ("the one full-state pass of each execute (input generated from the compact state of the "
+                         "leading passes; writes 16 B per amplitude)")
     achieved = bytes_per_pass / (avg_pass_ms / 1e3) / 1e9
-    exec_bytes = bytes_per_pass * passes_per_exec - (16.0 * (1 << n) if ppe > 1 else 0.0)
+    exec_bytes = 16.0 * (1 << n) + 32.0 * (1 << n) * (ppe - 1)
     # DRAM bytes per launch from the committed ncu summary (26-qubit capture
     # scaled by the amplitudes per launch), for the 30-qubit workload only
     traffic = None
     try:
-        with open(os.path.join(ROOT, "profiles", "qse_pass_hrz_qft_26q.md")) as f:
+        with open(os.path.join(ROOT, "profiles", f"{kernel}_hrz_qft_26q.md")) as f:
             for line in f:
                 if f"traffic_bytes_per_launch_{n}q:" in line:
                     traffic = float(line.split(":")[-1])
@@ -650,15 +663,18 @@ def main():
             "config": workload_config(n, ngates, args.shots),
             "parallelism": f"replicas{world}" if world > 1 else "single",
             "passes_per_execute": passes_per_exec,
+            "passes_per_execute_meaning": "passes over the full state (leading passes on a compact state not counted)",
             "phases": phases,
             "execute_ms": pass_ms / args.steps,
+            "execute_ms_meaning": "device time of the full-state passes of one execute (phases.execute_ms: the whole "
+                                  "execute)",
             "hbm_gbs_execute": exec_bytes / (pass_ms / args.steps / 1e3) / 1e9,
-            "zero_start_pass_ms": float(zs.mean()) if zs.size else None,
+            "first_pass_ms": float(zs.mean()) if zs.size else None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "qse_pass (fused pass, NVRTC-specialised)", "bytes_per_launch": bytes_per_pass,
+                         "kernel": f"{kernel} (fused pass, NVRTC-specialised)", "bytes_per_launch": bytes_per_pass,
                          "avg_launch_ms": avg_pass_ms,
-                         "launches": "read+write passes (2nd and 3rd of each execute)"},
+                         "launches": launches_desc},
             "e2e": {"value": e2e_value, "unit": "gates/s", "h2d_bytes_per_step": int(ops.nbytes),
                     "d2h_bytes_per_step": int(8 * args.shots + 8)},
             "gpu_launches": int(launches),

@@ -414,20 +414,85 @@ uint64_t run_fused(qse_state* st, const std::vector<plan::Gate>& gates)
 // state of only the touched qubits: 2^m amplitudes (at most 64 MiB, resident
 // in L2) instead of 2^n.  The first pass over the full state then reads its
 // input from that compact state (jit.cpp, compact input) instead of from HBM.
-// Untouched here means untouched by any gate, diagonal ones included, so the
-// compact circuit is the prefix's gates unchanged with its qubits renumbered.
+// Touched means acted on non-diagonally (a target other than of a phase, or a
+// SWAP); an untouched qubit keeps its basis bit through the prefix, so in the
+// prefix's diagonal gates and CNOT controls it is a known 0 or 1: those gates
+// drop, lose that qubit, or become a factor of the whole state (compact_gate).
 constexpr uint32_t kCompactMinQubits = 24;   // full states this large (smaller ones gain little)
 constexpr uint32_t kCompactMaxQubits = 22;   // compact states up to this size
 
-uint64_t gate_qubits(const plan::Gate& g)
+// qubits a gate acts on non-diagonally
+uint64_t gate_nondiag(const plan::Gate& g)
 {
     auto b = [](uint32_t q) { return uint64_t(1) << q; };
     switch (g.type) {
-    case QSE_GATE_IDENTITY: return 0;
-    case QSE_GATE_CNOT: case QSE_GATE_CPHASE: case QSE_GATE_SWAP: return b(g.t) | b(g.c);
-    case QSE_GATE_MCPHASE: return b(g.t) | g.cmask;
-    default: return b(g.t);
+    case QSE_GATE_H: case QSE_GATE_X: case QSE_GATE_Y: case QSE_GATE_RX: case QSE_GATE_RY: case QSE_GATE_2X2:
+        return b(g.t);
+    case QSE_GATE_CNOT: return g.c == g.t ? 0 : b(g.t);   // control == target: a no-op
+    case QSE_GATE_SWAP: return g.c == g.t ? 0 : b(g.t) | b(g.c);
+    default: return 0;   // identity and the phase gates
     }
+}
+
+// Gate g of the prefix on the compact state: qubits in `touched` renumbered by
+// rank, the others replaced by their basis bit (bit); a gate that becomes a
+// factor of the whole state multiplies glob instead.  Appends to out.
+void compact_gate(const plan::Gate& g, uint64_t touched, const uint32_t* rank, uint64_t bits,
+                  std::vector<plan::Gate>& out, double& gre, double& gim)
+{
+    auto in = [&](uint32_t q) { return (touched >> q) & 1; };
+    auto bit = [&](uint32_t q) { return (bits >> q) & 1; };
+    auto mul = [&](double c, double s) {
+        const double r = gre * c - gim * s, i = gre * s + gim * c;
+        gre = r;
+        gim = i;
+    };
+    plan::Gate x = g;
+    switch (g.type) {
+    case QSE_GATE_IDENTITY: return;
+    case QSE_GATE_Z: case QSE_GATE_PHASE: case QSE_GATE_RZ:
+        if (in(g.t)) break;
+        if (g.type == QSE_GATE_RZ) mul(std::cos(g.theta / 2), bit(g.t) ? std::sin(g.theta / 2) : -std::sin(g.theta / 2));
+        else if (bit(g.t)) {
+            if (g.type == QSE_GATE_Z) mul(-1.0, 0.0);
+            else mul(std::cos(g.theta), std::sin(g.theta));
+        }
+        return;
+    case QSE_GATE_CNOT:
+        if (g.c == g.t) return;
+        if (!in(g.c)) {   // a classical control: X on the target or nothing
+            if (!bit(g.c)) return;
+            x.type = QSE_GATE_X;
+        }
+        break;
+    case QSE_GATE_CPHASE: case QSE_GATE_MCPHASE: {
+        // phase theta on the amplitudes whose bits of `all` are all 1
+        uint64_t all = g.type == QSE_GATE_CPHASE ? ((uint64_t(1) << g.t) | (uint64_t(1) << g.c))
+                                                 : (g.cmask | (uint64_t(1) << g.t));
+        const uint64_t fixed = all & ~touched;
+        if (!fixed) break;                      // every qubit touched: the gate as it is
+        if ((fixed & bits) != fixed) return;   // a classical qubit at 0: never applies
+        all &= touched;
+        if (!all) {
+            mul(std::cos(g.theta), std::sin(g.theta));
+            return;
+        }
+        x.type = QSE_GATE_MCPHASE;
+        x.t = uint32_t(__builtin_ctzll(all));
+        x.cmask = all & (all - 1);
+        x.c = 0;
+        break;
+    }
+    default: break;
+    }
+    x.t = rank[x.t];
+    if (x.type == QSE_GATE_CNOT || x.type == QSE_GATE_CPHASE || x.type == QSE_GATE_SWAP) x.c = rank[x.c];
+    if (x.type == QSE_GATE_MCPHASE) {
+        uint64_t cm = 0;
+        for (uint64_t b = x.cmask; b; b &= b - 1) cm |= uint64_t(1) << rank[__builtin_ctzll(b)];
+        x.cmask = cm;
+    }
+    out.push_back(x);
 }
 
 qse_state* compact_state(qse_ctx* ctx, uint32_t m)
@@ -454,7 +519,9 @@ qse_state* compact_state(qse_ctx* ctx, uint32_t m)
 // touch at most kCompactMaxQubits qubits on the compact state and leaves st
 // in the lazy compact form; rest = the other gates in program order (a valid
 // order: every gate of the prefix passes runs before every other gate in the
-// plan).  False (nothing done) when no such prefix exists.
+// plan).  False (nothing done) when no such prefix exists.  A CPHASE or
+// MCPHASE that keeps only touched qubits becomes an MCPHASE on them (the same
+// phase on the same amplitudes).
 bool compact_prefix(qse_state* st, const std::vector<plan::Gate>& gates_in, std::vector<plan::Gate>& rest,
                     uint64_t& passes)
 {
@@ -471,12 +538,12 @@ bool compact_prefix(qse_state* st, const std::vector<plan::Gate>& gates_in, std:
     size_t K = 0;
     uint64_t u = 0, uK = 0;
     for (size_t i = 0; i < pl.passes.size(); ++i) {
-        for (uint32_t g : pl.passes[i].order) u |= gate_qubits(gates[g]);
+        for (uint32_t g : pl.passes[i].order) u |= gate_nondiag(gates[g]);
         if (uint32_t(__builtin_popcountll(u)) > kCompactMaxQubits) break;
         K = i + 1;
         uK = u;
     }
-    if (K < 2) return false;
+    if (K < 2 || uK == 0) return false;
     // compact qubit r = the touched qubit with the r-th lowest physical position
     std::vector<uint32_t> qs;
     for (uint32_t q = 0; q < st->n; ++q)
@@ -484,27 +551,31 @@ bool compact_prefix(qse_state* st, const std::vector<plan::Gate>& gates_in, std:
     std::sort(qs.begin(), qs.end(), [&](uint32_t a, uint32_t b) { return st->perm[a] < st->perm[b]; });
     const uint32_t m = uint32_t(qs.size());
     uint32_t rank[64] = {0};
-    uint64_t umask = 0, cbasis = 0;
+    uint64_t umask = 0, cbasis = 0, lbits = 0;   // lbits: basis bit of every logical qubit
+    for (uint32_t q = 0; q < st->n; ++q) lbits |= ((st->lazy_index >> st->perm[q]) & 1) << q;
     for (uint32_t r = 0; r < m; ++r) {
         rank[qs[r]] = r;
         umask |= uint64_t(1) << st->perm[qs[r]];
-        cbasis |= ((st->lazy_index >> st->perm[qs[r]]) & 1) << r;
+        cbasis |= ((lbits >> qs[r]) & 1) << r;
     }
     std::vector<char> in_prefix(gates.size(), 0);
     std::vector<plan::Gate> sub;
+    double gre = 1.0, gim = 0.0;
     for (size_t i = 0; i < K; ++i)
         for (uint32_t g : pl.passes[i].order) {
             in_prefix[g] = 1;
-            plan::Gate x = gates[g];
-            x.t = rank[x.t];
-            if (x.type == QSE_GATE_CNOT || x.type == QSE_GATE_CPHASE || x.type == QSE_GATE_SWAP) x.c = rank[x.c];
-            if (x.type == QSE_GATE_MCPHASE) {
-                uint64_t cm = 0;
-                for (uint64_t b = x.cmask; b; b &= b - 1) cm |= uint64_t(1) << rank[__builtin_ctzll(b)];
-                x.cmask = cm;
-            }
-            sub.push_back(x);
+            compact_gate(gates[g], uK, rank, lbits, sub, gre, gim);
         }
+    if (gre != 1.0 || gim != 0.0) {   // the factors of the classical qubits' phases
+        plan::Gate f{};
+        f.type = QSE_GATE_2X2;
+        f.t = 0;
+        f.m[0] = gre;
+        f.m[1] = gim;
+        f.m[6] = gre;
+        f.m[7] = gim;
+        sub.push_back(f);
+    }
     rest.clear();
     for (size_t g = 0; g < gates.size(); ++g)
         if (!in_prefix[g]) rest.push_back(gates[g]);

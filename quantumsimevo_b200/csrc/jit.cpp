@@ -100,6 +100,11 @@ struct Gen {
     // (lam, 2^popcount(umask) amplitudes indexed by those bits in ascending
     // order); the other qubits hold the bits of bi.  0: the plain basis state
     uint64_t umask = 0;
+    // kernel names tell the input kinds apart in profiles
+    std::string kernel_name() const
+    {
+        return !zero_in ? "qse_pass" : umask ? "qse_pass_compact_in" : "qse_pass_basis_in";
+    }
     bool xb_used = false;   // the exchange buffer holds data some thread may still read
     std::string SYNC = "__syncthreads();";   // barrier of the threads that share xb
     // gradient slots accumulated per thread (slot -> accumulator index)
@@ -542,7 +547,7 @@ struct Gen {
         src << "struct Prm { double v[" << std::max<size_t>(1, prm.size()) << "]; };\n";
         // resident CTAs per SM the register budget allows at 128 registers per thread
         const uint32_t min_blocks = std::max(1u, std::min(8u, 65536u / (T * 128u)));
-        src << "extern \"C\" __global__ void __launch_bounds__(" << T << ", " << min_blocks << ") qse_pass("
+        src << "extern \"C\" __global__ void __launch_bounds__(" << T << ", " << min_blocks << ") " << kernel_name() << "("
             << "double2* __restrict__ psi, double2* __restrict__ lam, const TermRec* __restrict__ terms, "
             << "const GroupRec* __restrict__ groups, double* __restrict__ slot_partial, u32* __restrict__ status, "
             << "const double2* __restrict__ gvt, const __grid_constant__ Prm P)\n{\n"
@@ -897,6 +902,7 @@ Source generate(const plan::PassProgram& p, int nstates, bool basis_input, bool 
     s.prm = std::move(g.prm);
     s.basis_slot = g.basis_slot;
     s.pre_gv = g.pre_gv;
+    s.name = g.kernel_name();
     s.ngroups = uint32_t(p.groups.size());
     s.threads = g.T;
     s.smem = (size_t(1) << p.k) * 16 + p.groups.size() * 16 + size_t(g.ntab) * 32 * 16 +
@@ -947,7 +953,7 @@ std::vector<std::shared_ptr<Kernel>> get_kernels(const std::vector<const Source*
         if (bins[w].empty()) fail(QSE_ERR_CUDA, "pass kernel compilation failed: " + errs[w]);
         auto k = std::make_shared<Kernel>();
         QSE_CUDA(cudaLibraryLoadData(&k->lib, bins[w].data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
-        QSE_CUDA(cudaLibraryGetKernel(&k->kern, k->lib, "qse_pass"));
+        QSE_CUDA(cudaLibraryGetKernel(&k->kern, k->lib, srcs[todo[w]]->name.c_str()));
         k->threads = srcs[todo[w]]->threads;
         g_cache[srcs[todo[w]]->code] = k;
     }

@@ -16,6 +16,7 @@ namespace jit {
 
 struct Source {
     std::string code;         // CUDA C++ of the pass kernel (angles not included)
+    std::string name = "qse_pass";   // its entry point (qse_pass, qse_pass_basis_in, qse_pass_compact_in)
     std::vector<double> prm;  // the kernel's parameter block (angles, matrices, scales)
     uint32_t threads = 0;
     size_t smem = 0;
