@@ -244,7 +244,7 @@ constexpr size_t kJitMaxNewKernels = 32;
 // use_jit = true) or, when the context disables them or they are not worth
 // compiling, for the interpreter (angle accumulators, use_jit = false).
 plan::Plan plan_for(qse_state* st, const std::vector<plan::Gate>& gates, plan::Options opt, int ns, bool& use_jit,
-                    std::vector<jit::Source>& srcs)
+                    std::vector<jit::Source>& srcs, bool prob_out = false)
 {
     use_jit = st->ctx->jit != 0;
     opt.acc_mul = use_jit;
@@ -252,10 +252,14 @@ plan::Plan plan_for(qse_state* st, const std::vector<plan::Gate>& gates, plan::O
     srcs.clear();
     if (!use_jit) return pl;
     srcs.reserve(pl.passes.size());
+    // the last pass may also write the probabilities in logical order
+    uint8_t lpos[64] = {0};
+    for (uint32_t q = 0; q < st->n; ++q) lpos[pl.perm_final[q]] = uint8_t(q);
     for (size_t i = 0; i < pl.passes.size(); ++i) {
         const bool basis_in = i == 0 && ns == 1 && st->lazy_basis;
+        const bool prob = prob_out && ns == 1 && i + 1 == pl.passes.size();
         srcs.push_back(jit::generate(pl.passes[i], ns, basis_in, st->ctx->jit == 2, st->n >= jit::kPreGroupQubits,
-                                     basis_in ? st->lazy_umask : 0));
+                                     basis_in ? st->lazy_umask : 0, prob ? lpos : nullptr));
     }
     if (st->n >= kJitAlwaysQubits || jit::count_uncached(srcs) <= kJitMaxNewKernels) return pl;
     use_jit = false;
@@ -387,22 +391,39 @@ plan::Options fused_options(const qse_ctx* ctx, uint32_t n)
 }
 
 // Forward passes of gates on st through the planner; returns the pass count.
-uint64_t run_fused(qse_state* st, const std::vector<plan::Gate>& gates)
+// prob_out: the last pass also writes the probabilities in logical order and
+// their block sums into the state's sampling buffer (specialised kernels,
+// states of at least one 4096-block).
+uint64_t run_fused(qse_state* st, const std::vector<plan::Gate>& gates, bool prob_out = false)
 {
     qse_ctx* ctx = st->ctx;
     bool use_jit = false;
     std::vector<jit::Source> srcs;
-    plan::Plan pl = plan_for(st, gates, fused_options(ctx, st->n), 1, use_jit, srcs);
+    prob_out = prob_out && st->size() >= 4096 && ctx->jit != 0;
+    plan::Plan pl = plan_for(st, gates, fused_options(ctx, st->n), 1, use_jit, srcs, prob_out);
     if (!use_jit) materialize(st);  // interpreter passes read the state
+    double* prob = nullptr;
+    const bool with_bsum = !srcs.empty() && srcs.back().prob_bsum;
+    if (prob_out && use_jit && !srcs.empty() && srcs.back().prob) {
+        st->cdf.reserve(prob_buffer_bytes(st->size()));
+        prob = static_cast<double*>(st->cdf.ptr);
+        QSE_CUDA(cudaMemsetAsync(prob + st->size(), 0, (st->size() / 4096) * 8, ctx->stream));
+        st->cdf_version = ~uint64_t(0);   // the buffer's cumulative values are overwritten
+    }
     Uploaded up = upload_plan(ctx, pl, use_jit && st->n >= jit::kPreGroupQubits);
     PassRunner runner(st, pl, up, 1, 4, use_jit, std::move(srcs));
-    for (size_t i = 0; i < up.args.size(); ++i) runner.run(i, nullptr, nullptr);
+    for (size_t i = 0; i < up.args.size(); ++i) runner.run(i, nullptr, i + 1 == up.args.size() ? prob : nullptr);
     if (!up.args.empty()) {   // the first pass wrote every amplitude
         st->lazy_basis = false;
         st->lazy_umask = 0;
         st->lazy_src = nullptr;
     }
     for (uint32_t q = 0; q < st->n; ++q) st->perm[q] = pl.perm_final[q];
+    if (prob) {
+        st->prob_version = st->version;
+        st->prob_pending = true;
+        st->prob_bsum = with_bsum;
+    }
     return pl.passes.size();
 }
 
@@ -639,13 +660,18 @@ void execute_program(qse_state* st, const qse_op* ops, size_t nops, const double
         for (const plan::Gate& g : gates) apply_plain(st, g);
         passes = gates.size();
     } else {
+        // probabilities for the sampler from the last pass: only while the
+        // state is being sampled (the last ones written were read) and no
+        // Pauli frame follows
+        if (st->prob_pending) st->prob_hint = st->prob_pending = false;
+        const bool prob_out = st->prob_hint && !(noise && noise->cfg.enabled);
         std::vector<plan::Gate> rest;
         uint64_t compact_passes = 0;
         if (compact_prefix(st, gates, rest, compact_passes)) {
-            passes = compact_passes + run_fused(st, rest);
+            passes = compact_passes + run_fused(st, rest, prob_out);
             materialize(st);   // no pass consumed the compact form (nothing after the prefix)
         } else {
-            passes = run_fused(st, gates);
+            passes = run_fused(st, gates, prob_out);
         }
     }
     if (noise && noise->cfg.enabled) launch_pauli_frame(st, noise->d_counts);

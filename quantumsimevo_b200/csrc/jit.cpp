@@ -100,6 +100,10 @@ struct Gen {
     // (lam, 2^popcount(umask) amplitudes indexed by those bits in ascending
     // order); the other qubits hold the bits of bi.  0: the plain basis state
     uint64_t umask = 0;
+    // probability side output (forward passes): logical position of every
+    // physical qubit after this pass; empty = none (emit_prob)
+    std::vector<uint8_t> lpos;
+    bool prob_bsum = false;   // the side output includes the block sums
     // kernel names tell the input kinds apart in profiles
     std::string kernel_name() const
     {
@@ -416,6 +420,7 @@ struct Gen {
             if (ns == 2) o << " lam[gb + " << hex(reg_off(j)) << "] = a1[" << j << "];";
             o << "\n";
         }
+        if (!lpos.empty()) emit_prob();
         for (const auto& kv : gacc)
             o << "  { const double v = warpSum<" << T << ">(gs" << kv.second << ");"
               << " if ((tid & 31u) == 0u) wp[" << kv.first << "u * " << NW << "u + (tid >> 5)] += v; }\n";
@@ -554,6 +559,123 @@ struct Gen {
             << "  (void)lam; (void)terms; (void)groups; (void)slot_partial; (void)status; (void)gvt;\n"
             << head.str() << ops_txt << "}\n";
         return src.str();
+    }
+
+    // Probability side output of the last pass of an execute: |a|^2 of every
+    // stored amplitude (re*re + im*im, two roundings, as the sampler computes
+    // it) into prob[logical index], and the sums of its logical 4096-blocks
+    // into bsum = prob + 2^n (zeroed before the pass; atomic adds, so their
+    // order varies, which only the sampler's binade guess sees).  The tile's
+    // values go through shared memory in "local" order (tile bits sorted by
+    // logical position) so that consecutive threads store consecutive logical
+    // indices.  An XOR of the lane bits that sit at local positions >= 4 into
+    // the free low positions keeps the scattered writes to shared memory at
+    // most two-way conflicted; the linear reads stay conflict-free.
+    void emit_prob()
+    {
+        const uint32_t n = P.k + uint32_t(__builtin_popcountll(P.outer_mask));
+        // local rank of every tile bit
+        std::vector<std::pair<int, uint32_t>> lp;
+        for (uint32_t b = 0; b < P.k; ++b) lp.push_back({lpos[P.tile_phys[b]], b});
+        std::sort(lp.begin(), lp.end());
+        uint32_t lr[16] = {0};
+        std::vector<int> lsorted(P.k);
+        for (uint32_t i = 0; i < P.k; ++i) {
+            lr[lp[i].second] = i;
+            lsorted[i] = lp[i].first;
+        }
+        // swizzle: lane bits at local positions >= 4 into the free low positions
+        const uint32_t nl = std::min<uint32_t>(5, uint32_t(nthr));
+        uint32_t lowused = 0;
+        std::vector<uint32_t> highlane;
+        for (uint32_t t = 0; t < nl; ++t) {
+            const uint32_t l = lr[thr[t]];
+            if (l < 4) lowused |= 1u << l;
+            else highlane.push_back(l);
+        }
+        std::string swz;
+        {
+            uint32_t slot = 0;
+            for (uint32_t l : highlane) {
+                while (slot < 4 && ((lowused >> slot) & 1)) ++slot;
+                if (slot >= 4) break;
+                swz += " ^ (((x >> " + std::to_string(l) + ") & 1u) << " + std::to_string(slot) + ")";
+                ++slot;
+            }
+        }
+        o << "  {\n    // probabilities in logical order and their 4096-block sums\n"
+          << "    double* const prob = slot_partial;\n"
+          << "    double* const bsum = prob + " << hex(uint64_t(1) << n) << ";\n"
+          << "    double* const pb = reinterpret_cast<double*>(xb);\n"
+          << "    auto sw = [](u32 x) { return x" << swz << "; };\n"
+          << "    __syncthreads();\n";
+        std::string ls = "0u";
+        for (int t = 0; t < nthr; ++t)
+            ls += " | (((tid >> " + std::to_string(t) + ") & 1u) << " + std::to_string(lr[thr[t]]) + ")";
+        o << "    const u32 ls = " << ls << ";\n";
+        for (uint32_t j = 0; j < R; ++j) {
+            uint32_t off = 0;
+            for (uint32_t i = 0; i < P.rb; ++i)
+                if ((j >> i) & 1) off |= 1u << lr[reg[i]];
+            o << "    pb[sw(ls | " << off << "u)] = __dadd_rn(__dmul_rn(a0[" << j << "].x, a0[" << j << "].x), __dmul_rn(a0["
+              << j << "].y, a0[" << j << "].y));\n";
+        }
+        o << "    __syncthreads();\n";
+        // logical base of the tile and of this thread's store index (tid + k*T)
+        o << "    u64 lb = 0;\n    { u64 c = blockIdx.x;";
+        for (uint32_t q = 0; q < 64; ++q)
+            if ((P.outer_mask >> q) & 1) o << " lb |= (c & 1ull) << " << int(lpos[q]) << "; c >>= 1;";
+        o << " (void)c; }\n";
+        const uint32_t lt = uint32_t(__builtin_ctz(T));
+        std::string lt_expr = "lb";
+        for (uint32_t i = 0; i < lt; ++i)
+            lt_expr += " | ((u64)((tid >> " + std::to_string(i) + ") & 1u) << " + std::to_string(lsorted[i]) + ")";
+        o << "    const u64 lbt = " << lt_expr << ";\n";
+        // block key of each k: the logical bits >= 12 of its local bits; the
+        // thread bits must all map below 12 for a per-CTA reduction
+        uint32_t i0 = P.k;
+        for (uint32_t i = 0; i < P.k; ++i)
+            if (lsorted[i] >= 12) { i0 = i; break; }
+        std::map<uint64_t, std::vector<uint32_t>> keys;
+        for (uint32_t kk = 0; kk < R; ++kk) {
+            uint64_t lk = 0;
+            for (uint32_t i = lt; i < P.k; ++i)
+                if (((uint64_t(kk) * T) >> i) & 1) lk |= uint64_t(1) << lsorted[i];
+            o << "    const double p" << kk << " = pb[sw(tid + " << kk * T << "u)]; prob[lbt | " << hex(lk) << "] = p" << kk
+              << ";\n";
+            keys[lk >> 12].push_back(kk);
+        }
+        prob_bsum = i0 >= 5;
+        if (i0 >= lt) {
+            // one sum per block key: per thread, per warp, then per CTA in shared memory
+            o << "    double* const bs = pb + " << (1u << P.k) << ";\n";
+            uint32_t ki = 0;
+            for (const auto& kv : keys) {
+                o << "    { double v = 0.0;";
+                for (uint32_t kk : kv.second) o << " v += p" << kk << ";";
+                o << " v = warpSum<" << T << ">(v); if ((tid & 31u) == 0u) bs[" << ki * NW << "u + (tid >> 5)] = v; }\n";
+                ++ki;
+            }
+            o << "    __syncthreads();\n";
+            ki = 0;
+            for (const auto& kv : keys) {
+                o << "    if (tid == " << ki << "u) { double v = 0.0; for (u32 w = 0; w < " << NW << "u; ++w) v += bs["
+                  << ki * NW << "u + w]; atomicAdd(bsum + ((lb >> 12) | " << hex(kv.first) << "), v); }\n";
+                ++ki;
+            }
+        } else if (prob_bsum) {
+            // warp bits at logical positions >= 12: one sum per warp and k
+            for (uint32_t kk = 0; kk < R; ++kk) {
+                uint64_t lk = 0;
+                for (uint32_t i = lt; i < P.k; ++i)
+                    if (((uint64_t(kk) * T) >> i) & 1) lk |= uint64_t(1) << lsorted[i];
+                o << "    { const double v = warpSum<" << T << ">(p" << kk << "); if ((tid & 31u) == 0u) atomicAdd(bsum + ((lbt | "
+                  << hex(lk) << ") >> 12), v); }\n";
+            }
+        }
+        // else: lane bits at logical positions >= 12 (a warp's 32 values span
+        // several blocks); the sampler sums the blocks from prob instead
+        o << "  }\n";
     }
 
     // ---- streamed pass (forward passes on large states) ----
@@ -882,9 +1004,9 @@ static bool streamable(const plan::PassProgram& p, int nstates, bool basis_input
 }
 
 Source generate(const plan::PassProgram& p, int nstates, bool basis_input, bool streamed, bool precomputed_groups,
-                uint64_t compact_mask)
+                uint64_t compact_mask, const uint8_t* prob_lpos)
 {
-    if (streamed && streamable(p, nstates, basis_input)) {
+    if (streamed && !prob_lpos && streamable(p, nstates, basis_input)) {
         Gen g(p, nstates, false);
         Source s;
         s.code = g.run_streamed();
@@ -897,12 +1019,17 @@ Source generate(const plan::PassProgram& p, int nstates, bool basis_input, bool 
         }
     }
     Gen g(p, nstates, basis_input, precomputed_groups, compact_mask);
+    // (not with a tile that stores zeros and returns early: a basis input with outer bits)
+    if (prob_lpos && nstates == 1 && !(g.zero_in && (p.outer_mask & ~g.umask) != 0))
+        g.lpos.assign(prob_lpos, prob_lpos + 64);
     Source s;
     s.code = g.run();
     s.prm = std::move(g.prm);
     s.basis_slot = g.basis_slot;
     s.pre_gv = g.pre_gv;
     s.name = g.kernel_name();
+    s.prob = !g.lpos.empty();
+    s.prob_bsum = g.prob_bsum;
     s.ngroups = uint32_t(p.groups.size());
     s.threads = g.T;
     s.smem = (size_t(1) << p.k) * 16 + p.groups.size() * 16 + size_t(g.ntab) * 32 * 16 +

@@ -17,6 +17,8 @@ namespace jit {
 struct Source {
     std::string code;         // CUDA C++ of the pass kernel (angles not included)
     std::string name = "qse_pass";   // its entry point (qse_pass, qse_pass_basis_in, qse_pass_compact_in)
+    bool prob = false;               // writes the probability side output (prob_lpos)
+    bool prob_bsum = false;          // ... with its 4096-block sums
     std::vector<double> prm;  // the kernel's parameter block (angles, matrices, scales)
     uint32_t threads = 0;
     size_t smem = 0;
@@ -57,8 +59,12 @@ size_t compile_only(const Source& s);
 // compact_mask (with basis_input): the input is a compact state on the
 // physical qubits of the mask (passed as `lam` at launch, indexed by those
 // bits in ascending order) times the basis bits of i on the other qubits
+// prob_lpos (forward passes): the pass also writes the probabilities of the
+// amplitudes it stores in logical order and their 4096-block sums (passed as
+// `slot_partial` at launch: 2^n doubles, then 2^n / 4096 sums, zeroed before);
+// prob_lpos[q] = logical position of physical qubit q after the pass
 Source generate(const plan::PassProgram& p, int nstates, bool basis_input = false, bool streamed = false,
-                bool precomputed_groups = false, uint64_t compact_mask = 0);
+                bool precomputed_groups = false, uint64_t compact_mask = 0, const uint8_t* prob_lpos = nullptr);
 // distinct sources among srcs that are not compiled yet
 size_t count_uncached(const std::vector<Source>& srcs);
 // compiled kernels for every source (cached by source text; missing ones are compiled in parallel)

@@ -99,6 +99,15 @@ struct qse_state {
     // ascending order) times the basis bits of lazy_index on the other qubits
     uint64_t lazy_umask = 0;
     const void* lazy_src = nullptr;
+    // probabilities written by the last pass of an execute (cdf buffer, see
+    // prob_buffer_bytes) are current while prob_version == version.  prob_hint:
+    // the state has been sampled, so executes write them; prob_pending: they
+    // were written and no sampling has read them yet (an execute that finds
+    // them unread stops writing them)
+    bool prob_hint = false;
+    bool prob_pending = false;
+    bool prob_bsum = false;      // the block sums were written with them
+    uint64_t prob_version = ~uint64_t(0);
     // exact cumulative probabilities (sample.cu), valid while cdf_version == version
     qse::DevBuf cdf;
     uint64_t cdf_version = ~uint64_t(0);
@@ -174,6 +183,7 @@ void execute_program(qse_state* st, const qse_op* ops, size_t nops, const double
 void canonicalize(qse_state* st);
 
 // ---- sampling (sample.cu) ----
+size_t prob_buffer_bytes(uint64_t size);
 void sample(qse_state* st, const double* u_host, size_t nshots, uint64_t seed, uint64_t* out_host);
 void sample_device(qse_state* st, const double* d_u, size_t nshots, uint64_t seed, uint64_t* d_out);
 uint64_t measure(qse_state* st, double u);

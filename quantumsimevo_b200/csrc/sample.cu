@@ -462,6 +462,16 @@ __device__ __forceinline__ void block_sum_store(double s, double* out)
     }
 }
 
+// Block sums of a probability array written without them (coalesced reads).
+__global__ void __launch_bounds__(kBT) k_block_sums(const double* __restrict__ prob, double* __restrict__ bsum)
+{
+    const double* src = prob + uint64_t(blockIdx.x) * kBS + threadIdx.x;
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < kEPT; ++j) s += src[j * kBT];
+    block_sum_store(s, bsum + blockIdx.x);
+}
+
 // Identity qubit map: prob[i] = |amp[i]|^2 (coalesced), block sums on the way.
 __global__ void __launch_bounds__(kBT) k_prob_identity(const double2* __restrict__ amp, double* __restrict__ prob,
                                                        double* __restrict__ bsum)
@@ -1330,6 +1340,10 @@ CdfView build_cdf(qse_state* st)
     materialize(st);
     qse_ctx* ctx = st->ctx;
     const uint64_t size = st->size();
+    // this state is sampled: its next executes also write the probabilities
+    // (the last pass's side output), which this call consumes if they are current
+    st->prob_hint = true;
+    st->prob_pending = false;
     if (st->cdf_version == st->version)
         return CdfView{st->cdf_values, st->cdf_block_start, st->cdf_nb, st->cdf_bs};
     PermMap pm = make_perm(st);
@@ -1346,23 +1360,29 @@ CdfView build_cdf(qse_state* st)
         count_launch(ctx);
     } else {
         const uint32_t nb = uint32_t(size / kBS);
-        // state-owned: cdf [size] | cin [nb+1];  context scratch: bsum [nb] | guess [nb] | summ [nb] | group sums
-        st->cdf.reserve(size * 8 + (size_t(nb) + 1) * 8 + 16);
+        // state-owned: probabilities [size] | bsum [nb] | cin [nb+1] | stats;
+        // context scratch: guess [nb] | summ [nb] | group sums
+        st->cdf.reserve(prob_buffer_bytes(size));
         v.cdf = static_cast<double*>(st->cdf.ptr);
-        v.cin = v.cdf + size;
-        size_t off_guess = size_t(nb) * 8;
-        size_t off_summ = (off_guess + size_t(nb) * 4 + 15) & ~size_t(15);
+        double* bsum = v.cdf + size;
+        v.cin = bsum + nb;
+        size_t off_summ = (size_t(nb) * 4 + 15) & ~size_t(15);
         size_t off_gtot = off_summ + size_t(nb) * sizeof(Summ);
         ctx->scratch2.reserve(off_gtot + (size_t(nb) / kGT + 1) * 8);
         char* base = static_cast<char*>(ctx->scratch2.ptr);
-        double* bsum = reinterpret_cast<double*>(base);
-        int32_t* guess = reinterpret_cast<int32_t*>(base + off_guess);
+        int32_t* guess = reinterpret_cast<int32_t*>(base);
         Summ* summ = reinterpret_cast<Summ*>(base + off_summ);
         double* gtot = reinterpret_cast<double*>(base + off_gtot);
         v.nb = nb;
         v.bs = kBS;
-        // probabilities in logical order into the cumulative array (transformed in place below)
-        if (pm.identity) {
+        // probabilities in logical order and the block sums: written by the
+        // execute's last pass when current (prob_version), else gathered here
+        if (st->prob_version == st->version) {
+            if (!st->prob_bsum) {
+                k_block_sums<<<nb, kBT, 0, ctx->stream>>>(v.cdf, bsum);
+                count_launch(ctx);
+            }
+        } else if (pm.identity) {
             k_prob_identity<<<nb, kBT, 0, ctx->stream>>>(amp, v.cdf, bsum);
             count_launch(ctx);
         } else {
@@ -1502,6 +1522,16 @@ double total_probability(qse_state* st)
     return t;
 }
 
+}  // namespace qse
+
+namespace qse {
+// the state's sampling buffer: probabilities [size] | block sums [size/4096] |
+// exact block starts [size/4096 + 1] | scan statistics (16 B)
+size_t prob_buffer_bytes(uint64_t size)
+{
+    const size_t nb = size_t(size / kBS);
+    return size_t(size) * 8 + nb * 8 + (nb + 1) * 8 + 16;
+}
 }  // namespace qse
 
 namespace qse {
