@@ -301,14 +301,9 @@ int qse_state_create(qse_ctx* ctx, uint32_t nqubits, qse_state** out)
         delete st;
         qse::fail(QSE_ERR_OOM, "device allocation of the state vector failed (" + std::to_string(nqubits) + " qubits)");
     }
-    try {
-        qse::launch_init_zero_state(st);
-        QSE_CUDA(cudaStreamSynchronize(ctx->stream));
-    } catch (...) {
-        cudaFree(st->amp);
-        delete st;
-        throw;
-    }
+    // |0..0> recorded, not written: the first execute's first pass generates
+    // it, every other reader writes it first (materialize)
+    qse::mark_zero(st);
     *out = st;
     QSE_GUARD_END
 }

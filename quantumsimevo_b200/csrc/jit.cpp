@@ -646,16 +646,46 @@ struct Gen {
             keys[lk >> 12].push_back(kk);
         }
         prob_bsum = i0 >= 5;
-        if (i0 >= lt) {
-            // one sum per block key: per thread, per warp, then per CTA in shared memory
+        if (i0 >= lt && T >= 32) {
+            // one sum per block key: per thread, then across the warp by a
+            // transpose-reduce butterfly (each exchange halves the values a lane
+            // holds: 2K - 1 + 5 - log2 K shuffles for K keys instead of 5K), then
+            // per CTA in shared memory
             o << "    double* const bs = pb + " << (1u << P.k) << ";\n";
+            uint32_t K = 1;
+            while (K < keys.size()) K <<= 1;
+            o << "    {\n";
             uint32_t ki = 0;
             for (const auto& kv : keys) {
-                o << "    { double v = 0.0;";
-                for (uint32_t kk : kv.second) o << " v += p" << kk << ";";
-                o << " v = warpSum<" << T << ">(v); if ((tid & 31u) == 0u) bs[" << ki * NW << "u + (tid >> 5)] = v; }\n";
+                o << "      double v" << ki << " = 0.0;";
+                for (uint32_t kk : kv.second) o << " v" << ki << " += p" << kk << ";";
+                o << "\n";
                 ++ki;
             }
+            for (; ki < K; ++ki) o << "      double v" << ki << " = 0.0;\n";
+            uint32_t c = K, keymask = 0;
+            std::vector<std::pair<uint32_t, uint32_t>> keybits;   // (lane bit, key bit value)
+            for (uint32_t off = 16; off >= 1; off >>= 1) {
+                if (c > 1) {
+                    const uint32_t h = c / 2;
+                    o << "      { const bool hi = (tid & " << off << "u) != 0u;";
+                    for (uint32_t i = 0; i < h; ++i)
+                        o << " { const double s = hi ? v" << i << " : v" << i + h << "; const double k = hi ? v" << i + h
+                          << " : v" << i << "; v" << i << " = k + __shfl_xor_sync(0xffffffffu, s, " << off << "); }";
+                    o << " }\n";
+                    keybits.push_back({off, h});
+                    c = h;
+                } else {
+                    o << "      v0 += __shfl_xor_sync(0xffffffffu, v0, " << off << ");\n";
+                    keymask |= off;
+                }
+            }
+            std::string key = "0u";
+            for (const auto& kb : keybits) key += " + (((tid & " + std::to_string(kb.first) + "u) != 0u) ? " +
+                                                  std::to_string(kb.second) + "u : 0u)";
+            o << "      const u32 key = " << key << ";\n"
+              << "      if ((tid & " << keymask << "u) == 0u && key < " << keys.size() << "u) bs[key * " << NW
+              << "u + (tid >> 5)] = v0;\n    }\n";
             o << "    __syncthreads();\n";
             ki = 0;
             for (const auto& kv : keys) {
