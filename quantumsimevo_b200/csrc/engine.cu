@@ -540,7 +540,8 @@ qse_state* compact_state(qse_ctx* ctx, uint32_t m)
 // touch at most kCompactMaxQubits qubits on the compact state and leaves st
 // in the lazy compact form; rest = the other gates in program order (a valid
 // order: every gate of the prefix passes runs before every other gate in the
-// plan).  False (nothing done) when no such prefix exists.  A CPHASE or
+// plan, and both parts keep their program order, which the plan's order only
+// changes between gates that commute).  False (nothing done) when no such prefix exists.  A CPHASE or
 // MCPHASE that keeps only touched qubits becomes an MCPHASE on them (the same
 // phase on the same amplitudes).
 bool compact_prefix(qse_state* st, const std::vector<plan::Gate>& gates_in, std::vector<plan::Gate>& rest,
@@ -583,10 +584,11 @@ bool compact_prefix(qse_state* st, const std::vector<plan::Gate>& gates_in, std:
     std::vector<plan::Gate> sub;
     double gre = 1.0, gim = 0.0;
     for (size_t i = 0; i < K; ++i)
-        for (uint32_t g : pl.passes[i].order) {
-            in_prefix[g] = 1;
-            compact_gate(gates[g], uK, rank, lbits, sub, gre, gim);
-        }
+        for (uint32_t g : pl.passes[i].order) in_prefix[g] = 1;
+    // the prefix's gates in program order (a pass lists its SWAPs first: they
+    // only relabel there, but on the compact state they run where they stand)
+    for (size_t g = 0; g < gates.size(); ++g)
+        if (in_prefix[g]) compact_gate(gates[g], uK, rank, lbits, sub, gre, gim);
     if (gre != 1.0 || gim != 0.0) {   // the factors of the classical qubits' phases
         plan::Gate f{};
         f.type = QSE_GATE_2X2;
