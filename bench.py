@@ -589,12 +589,14 @@ def main():
         kernel = "qse_pass"
         launches_desc = "read+write full-state passes (all but the first of each execute)"
     else:
-        bytes_per_pass, avg_pass_ms = 16.0 * (1 << n), float(zs.mean())
+        # the steps sample, so the pass also writes each probability (8 B per
+        # amplitude) for the next sample
+        bytes_per_pass, avg_pass_ms = 24.0 * (1 << n), float(zs.mean())
         kernel = "qse_pass_compact_in"
         launches_desc = ("the one full-state pass of each execute (input generated from the compact state of the "
-                         "leading passes; writes 16 B per amplitude)")
+                         "leading passes; writes 16 B per amplitude and 8 B per probability for the sampler)")
     achieved = bytes_per_pass / (avg_pass_ms / 1e3) / 1e9
-    exec_bytes = 16.0 * (1 << n) + 32.0 * (1 << n) * (ppe - 1)
+    exec_bytes = 24.0 * (1 << n) + 32.0 * (1 << n) * (ppe - 1)
     # DRAM bytes per launch from the committed ncu summary (26-qubit capture
     # scaled by the amplitudes per launch), for the 30-qubit workload only
     traffic = None

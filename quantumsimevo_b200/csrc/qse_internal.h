@@ -59,7 +59,7 @@ struct qse_ctx {
     int max_gates_per_pass = 0;
     int sample_mode = 0;
     uint64_t launches = 0;
-    // device error word of the pass kernels (bounded waits that gave up):
+    // device error word of the kernels with bounded waits (streamed passes, the sampling scan):
     // mapped pinned host memory, read on the host after a synchronisation
     unsigned* status_host = nullptr;
     unsigned* status_dev = nullptr;
@@ -149,8 +149,8 @@ inline void check_device_status(qse_ctx* ctx)
     const unsigned v = *s;
     if (v == 0u) return;
     *s = 0u;
-    fail(QSE_ERR_TIMEOUT, "a pass kernel's bounded wait gave up (status " + std::to_string(v) +
-                              "); the state's amplitudes are invalid");
+    fail(QSE_ERR_TIMEOUT, "a kernel's bounded wait gave up (status " + std::to_string(v) +
+                              ": 1-2 a streamed pass, 4 the sampling scan); its results are invalid");
 }
 
 // ---- per-gate ("plain method") kernels: gates.cu ----

@@ -804,20 +804,53 @@ __global__ void __launch_bounds__(kBT, 4) k_cdf_summ(const double* __restrict__ 
 // start 45 8-byte words apart, so 16 threads hit 16 distinct bank pairs)
 constexpr int kChainPer = 9;
 constexpr uint32_t kSpan = uint32_t(kChainPer) * kBT;
-// dynamic shared memory of k_cdf_chain: two spans of fold records
-constexpr size_t kChainSmem = 2 * size_t(kSpan) * sizeof(Summ);
-static_assert(sizeof(Summ) % 8 == 0, "fold records are copied as 8-byte words");
+// one buffer of k_cdf_chain: a span of fold records copied from a 16-byte
+// aligned start (the records start 0 or 8 bytes in), rounded up to 16 bytes
+constexpr uint32_t kSpanBuf = uint32_t((size_t(kSpan) * sizeof(Summ) + 32) & ~size_t(15));
+constexpr size_t kChainSmem = 2 * size_t(kSpanBuf);
+// bytes after the fold records that a rounded-up copy may read (the
+// scratch that holds them reserves that much beyond them)
+constexpr size_t kSummSlack = 32;
+// polls of a bounded wait in k_cdf_chain before it gives up (status 4)
+constexpr uint32_t kChainWaitLimit = 1u << 22;
+static_assert(sizeof(Summ) % 8 == 0, "fold records are 8-byte aligned");
 
-// The fold records summ[base, base + cnt) into shared memory by 8-byte
-// asynchronous copies, committed as one group.
-__device__ __forceinline__ void summ_prefetch(Summ* dst, const Summ* src, uint32_t base, uint32_t cnt)
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+// The fold records summ[base, base + cnt) into buffer buf by bulk copies
+// (thread 0; completion counted on bar).  Returns the records' offset in buf.
+__device__ __forceinline__ uint32_t summ_fetch(char* buf, const Summ* summ, uint32_t base, uint32_t cnt, uint64_t* bar)
 {
-    const uint64_t* s = reinterpret_cast<const uint64_t*>(src + base);
-    const uint32_t d = uint32_t(__cvta_generic_to_shared(dst));
-    const uint32_t words = cnt * uint32_t(sizeof(Summ) / 8);
-    for (uint32_t i = threadIdx.x; i < words; i += kBT)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d + 8 * i), "l"(s + i) : "memory");
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    const uint64_t s0 = uint64_t(base) * sizeof(Summ);
+    const uint64_t a0 = s0 & ~uint64_t(15);
+    const uint32_t skew = uint32_t(s0 - a0);
+    const uint32_t bytes = (cnt * uint32_t(sizeof(Summ)) + skew + 15u) & ~15u;
+    const char* src = reinterpret_cast<const char*>(summ) + a0;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // earlier reads of buf before the copy's writes
+    asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes) : "memory");
+    constexpr uint32_t kPiece = 32768;
+    for (uint32_t o = 0; o < bytes; o += kPiece) {
+        const uint32_t nbytes = min(kPiece, bytes - o);
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_addr(buf + o)),
+                     "l"(src + o), "r"(nbytes), "r"(smem_addr(bar)) : "memory");
+    }
+    return skew;
+}
+
+// waits (every thread) for the phase of bar with the given parity; false
+// after kChainWaitLimit polls
+__device__ __forceinline__ bool chain_wait(uint64_t* bar, uint32_t parity)
+{
+    const uint32_t a = smem_addr(bar);
+    for (uint32_t i = 0; i < kChainWaitLimit; ++i) {
+        uint32_t done;
+        asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                     : "=r"(done) : "r"(a), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
 }
 
 // Single CTA: the exact running sum block by block.  cin[b] = exact sum
@@ -831,41 +864,61 @@ __device__ __forceinline__ void summ_prefetch(Summ* dst, const Summ* src, uint32
 // without a fold).  That block is handled on its own (its fold on the binade
 // it actually starts in, else an exact element-by-element fold) and the next
 // span starts after it.  The fold records of a span arrive in shared memory
-// while the previous span is composed (two buffers; a span that stopped early
-// reloads its successor's records).
+// by bulk copies while the previous span is composed (two buffers; a span
+// that stopped early reloads its successor's records).  Every wait on a copy
+// is bounded: one that gives up writes 4 to *status and the CTA stops, after
+// a bounded wait for the copies still in flight.
 __global__ void __launch_bounds__(kBT, 1) k_cdf_chain(const double* __restrict__ prob,
                                                    const Summ* __restrict__ summ, uint32_t nb, double* __restrict__ cin,
-                                                   uint32_t* __restrict__ stats)
+                                                   uint32_t* __restrict__ stats, unsigned* __restrict__ status)
 {
-    extern __shared__ Summ sbuf[];
+    extern __shared__ __align__(16) char sraw[];
     __shared__ uint64_t sh[160];
     __shared__ double stage[kBT * kPad];
     __shared__ double s_c;
     __shared__ int s_slow;
     __shared__ uint32_t s_end;
+    __shared__ __align__(8) uint64_t s_bar[2];
+    __shared__ uint32_t s_skew[2];
     uint32_t n_span = 0, n_single = 0, n_exact = 0;  // statistics (thread 0)
     const uint32_t t = threadIdx.x;
-    if (t == 0) s_c = 0.0;
-    uint32_t base = 0, loaded = 0, cur = 0;   // buffer cur holds the records from `loaded` on
-    summ_prefetch(sbuf, summ, 0, min(kSpan, nb));
+    uint32_t pend[2] = {0, 0}, ph[2] = {0, 0};   // copy in flight / parity of its phase, per buffer
+    uint32_t loaded[2] = {0, 0};
+    auto fetch = [&](uint32_t b, uint32_t from, uint32_t cnt) {   // every thread calls it (uniform state)
+        if (t == 0) s_skew[b] = summ_fetch(sraw + b * kSpanBuf, summ, from, cnt, &s_bar[b]);
+        pend[b] = 1;
+        loaded[b] = from;
+    };
+    auto drain = [&](uint32_t b) {   // wait for buffer b's copy; uniform result (a copy not seen done stays pending)
+        bool ok = true;
+        if (pend[b]) ok = chain_wait(&s_bar[b], ph[b]);
+        ok = __syncthreads_and(ok) != 0;
+        if (pend[b] && ok) {
+            ph[b] ^= 1u;
+            pend[b] = 0;
+        }
+        return ok;
+    };
+    if (t == 0) {
+        s_c = 0.0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s_bar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s_bar[1])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     __syncthreads();
+    uint32_t base = 0, cur = 0;
+    fetch(0, 0, min(kSpan, nb));
+    bool failed = false;
     while (base < nb) {
         const uint32_t span = min(kSpan, nb - base);
-        if (loaded != base) {   // the previous span stopped early: its successor's records
-            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-            __syncthreads();
-            summ_prefetch(sbuf + cur * kSpan, summ, base, span);
-            loaded = base;
+        if (loaded[cur] != base) {   // the previous span stopped early: its successor's records
+            if (!drain(0) || !drain(1)) { failed = true; break; }
+            fetch(cur, base, span);
         }
         const uint32_t next = base + span;
-        if (next < nb) {
-            summ_prefetch(sbuf + (cur ^ 1) * kSpan, summ, next, min(kSpan, nb - next));
-            asm volatile("cp.async.wait_group 1;\n" ::: "memory");
-        } else {
-            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        }
-        __syncthreads();
-        const Summ* rec = sbuf + cur * kSpan;
+        if (next < nb) fetch(cur ^ 1, next, min(kSpan, nb - next));
+        if (!drain(cur)) { failed = true; break; }
+        const Summ* rec = reinterpret_cast<const Summ*>(sraw + cur * kSpanBuf + s_skew[cur]);
         const double c = s_c;
         const int e0 = epoch_of(c);
         const uint32_t p0 = t * kChainPer;           // this thread's first position in the span
@@ -923,8 +976,7 @@ __global__ void __launch_bounds__(kBT, 1) k_cdf_chain(const double* __restrict__
         __syncthreads();   // every thread is done with rec and s_c before either changes
         if (end >= span) {
             base = next;
-            loaded = next;
-            cur ^= 1;
+            cur ^= 1;   // loaded[cur] == next: fetched above
             continue;
         }
         // block b starts in the running sum's binade but has no fold there or leaves it
@@ -957,7 +1009,12 @@ __global__ void __launch_bounds__(kBT, 1) k_cdf_chain(const double* __restrict__
         __syncthreads();
         base = b + 1;
     }
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    // no copy may still be writing shared memory when the CTA leaves
+    const bool d0 = drain(0), d1 = drain(1), drained = d0 && d1;
+    if (failed || !drained) {
+        if (t == 0) *(volatile unsigned*)status = 4u;
+        return;
+    }
     if (t == 0) {
         cin[nb] = s_c;
         if (stats) {
@@ -1368,7 +1425,7 @@ CdfView build_cdf(qse_state* st)
         v.cin = bsum + nb;
         size_t off_summ = (size_t(nb) * 4 + 15) & ~size_t(15);
         size_t off_gtot = off_summ + size_t(nb) * sizeof(Summ);
-        ctx->scratch2.reserve(off_gtot + (size_t(nb) / kGT + 1) * 8);
+        ctx->scratch2.reserve(off_gtot + (size_t(nb) / kGT + 1) * 8 + kSummSlack);
         char* base = static_cast<char*>(ctx->scratch2.ptr);
         int32_t* guess = reinterpret_cast<int32_t*>(base);
         Summ* summ = reinterpret_cast<Summ*>(base + off_summ);
@@ -1397,7 +1454,7 @@ CdfView build_cdf(qse_state* st)
         k_cdf_summ<<<nb, kBT, 0, ctx->stream>>>(v.cdf, guess, summ);
         QSE_CUDA(cudaFuncSetAttribute(k_cdf_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kChainSmem)));
         k_cdf_chain<<<1, kBT, kChainSmem, ctx->stream>>>(v.cdf, summ, nb, v.cin,
-                                                        reinterpret_cast<uint32_t*>(v.cin + nb + 1));
+                                                        reinterpret_cast<uint32_t*>(v.cin + nb + 1), ctx->status_dev);
         QSE_CUDA(cudaGetLastError());
         count_launch(ctx, 4);
         // the array keeps the probabilities: shots rebuild the cumulative values
