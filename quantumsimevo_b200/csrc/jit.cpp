@@ -107,6 +107,7 @@ struct Gen {
     // kernel names tell the input kinds apart in profiles
     std::string kernel_name() const
     {
+        if (ns == 2) return "qse_pass_adjoint";
         return !zero_in ? "qse_pass" : umask ? "qse_pass_compact_in" : "qse_pass_basis_in";
     }
     bool xb_used = false;   // the exchange buffer holds data some thread may still read

@@ -16,7 +16,7 @@ namespace jit {
 
 struct Source {
     std::string code;         // CUDA C++ of the pass kernel (angles not included)
-    std::string name = "qse_pass";   // its entry point (qse_pass, qse_pass_basis_in, qse_pass_compact_in)
+    std::string name = "qse_pass";   // its entry point (qse_pass, qse_pass_basis_in, qse_pass_compact_in, qse_pass_adjoint)
     bool prob = false;               // writes the probability side output (prob_lpos)
     bool prob_bsum = false;          // ... with its 4096-block sums
     std::vector<double> prm;  // the kernel's parameter block (angles, matrices, scales)

@@ -853,73 +853,80 @@ __device__ __forceinline__ bool chain_wait(uint64_t* bar, uint32_t parity)
     return false;
 }
 
-// Single CTA: the exact running sum block by block.  cin[b] = exact sum
-// before block b; cin[nb] = total.  A running sum of zero is on the grid of
-// binade -1022 (spacing 2^-1074, shared by the subnormals), where zero and
-// subnormal blocks fold exactly, so leading zero blocks take the fast path.
-// Each step takes the next span of up to kSpan blocks (kChainPer consecutive
-// per thread): every block up to the first one without a fold on the running
-// sum's binade composes with one block-wide scan, and the step commits the
-// blocks up to the first one whose sum would leave the binade (or the one
-// without a fold).  That block is handled on its own (its fold on the binade
-// it actually starts in, else an exact element-by-element fold) and the next
-// span starts after it.  The fold records of a span arrive in shared memory
-// by bulk copies while the previous span is composed (two buffers; a span
-// that stopped early reloads its successor's records).  Every wait on a copy
-// is bounded: one that gives up writes 4 to *status and the CTA stops, after
-// a bounded wait for the copies still in flight.
-__global__ void __launch_bounds__(kBT, 1) k_cdf_chain(const double* __restrict__ prob,
-                                                   const Summ* __restrict__ summ, uint32_t nb, double* __restrict__ cin,
-                                                   uint32_t* __restrict__ stats, unsigned* __restrict__ status)
-{
-    extern __shared__ __align__(16) char sraw[];
-    __shared__ uint64_t sh[160];
-    __shared__ double stage[kBT * kPad];
-    __shared__ double s_c;
-    __shared__ int s_slow;
-    __shared__ uint32_t s_end;
-    __shared__ __align__(8) uint64_t s_bar[2];
-    __shared__ uint32_t s_skew[2];
-    uint32_t n_span = 0, n_single = 0, n_exact = 0;  // statistics (thread 0)
-    const uint32_t t = threadIdx.x;
-    uint32_t pend[2] = {0, 0}, ph[2] = {0, 0};   // copy in flight / parity of its phase, per buffer
-    uint32_t loaded[2] = {0, 0};
-    auto fetch = [&](uint32_t b, uint32_t from, uint32_t cnt) {   // every thread calls it (uniform state)
-        if (t == 0) s_skew[b] = summ_fetch(sraw + b * kSpanBuf, summ, from, cnt, &s_bar[b]);
+// Shared memory of the chain (one CTA) besides the two record buffers.
+struct ChainShm {
+    uint64_t sh[160];
+    double stage[kBT * kPad];
+    double c;          // the exact running sum
+    int slow;
+    uint32_t end;
+    __align__(8) uint64_t bar[2];
+    uint32_t skew[2];
+};
+
+// The record buffers and their copies.  Every thread holds the same copy of
+// this state and calls fetch/drain together.
+struct ChainIO {
+    ChainShm& S;
+    char* raw;
+    const Summ* summ;
+    uint32_t pend[2] = {0, 0};             // copy in flight, per buffer
+    uint32_t ph[2] = {0, 0};               // parity of its mbarrier phase
+    uint32_t loaded[2] = {~0u, ~0u};       // first block the buffer holds (or will)
+    __device__ ChainIO(ChainShm& s, char* r, const Summ* sm) : S(s), raw(r), summ(sm) {}
+    __device__ void fetch(uint32_t b, uint32_t from, uint32_t cnt)
+    {
+        if (threadIdx.x == 0) S.skew[b] = summ_fetch(raw + b * kSpanBuf, summ, from, cnt, &S.bar[b]);
         pend[b] = 1;
         loaded[b] = from;
-    };
-    auto drain = [&](uint32_t b) {   // wait for buffer b's copy; uniform result (a copy not seen done stays pending)
+    }
+    // waits for buffer b's copy; uniform result (a copy not seen done stays pending)
+    __device__ bool drain(uint32_t b)
+    {
         bool ok = true;
-        if (pend[b]) ok = chain_wait(&s_bar[b], ph[b]);
+        if (pend[b]) ok = chain_wait(&S.bar[b], ph[b]);
         ok = __syncthreads_and(ok) != 0;
         if (pend[b] && ok) {
             ph[b] ^= 1u;
             pend[b] = 0;
         }
         return ok;
-    };
-    if (t == 0) {
-        s_c = 0.0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s_bar[0])) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s_bar[1])) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    __syncthreads();
-    uint32_t base = 0, cur = 0;
-    fetch(0, 0, min(kSpan, nb));
-    bool failed = false;
-    while (base < nb) {
-        const uint32_t span = min(kSpan, nb - base);
-        if (loaded[cur] != base) {   // the previous span stopped early: its successor's records
-            if (!drain(0) || !drain(1)) { failed = true; break; }
-            fetch(cur, base, span);
+    __device__ const Summ* rec(uint32_t b) const { return reinterpret_cast<const Summ*>(raw + b * kSpanBuf + S.skew[b]); }
+};
+
+// The exact running sum over blocks [b_begin, b_end), starting from S.c (the
+// exact sum before b_begin) and leaving the sum after b_end there; writes
+// cin[b_begin, b_end).  Each step takes the next span of up to kSpan blocks
+// (kChainPer consecutive per thread): every block up to the first one without
+// a fold on the running sum's binade composes with one block-wide scan, and
+// the step commits the blocks up to the first one whose sum would leave the
+// binade (or the one without a fold).  That block is handled on its own (its
+// fold on the binade it actually starts in, else an exact element-by-element
+// fold) and the next span starts after it.  The fold records of a span arrive
+// in shared memory by bulk copies while the previous span is composed (two
+// buffers; a span that stopped early reloads its successor's records; records
+// already in buffer 0 for b_begin are used as they are).  A running sum of
+// zero is on the grid of binade -1022 (spacing 2^-1074, shared by the
+// subnormals), where zero and subnormal blocks fold exactly.  False when a
+// bounded wait gave up.
+__device__ bool chain_range(ChainIO& io, const double* __restrict__ prob, uint32_t b_begin, uint32_t b_end,
+                            double* __restrict__ cin, uint32_t& n_span, uint32_t& n_single, uint32_t& n_exact)
+{
+    ChainShm& S = io.S;
+    const uint32_t t = threadIdx.x;
+    uint32_t base = b_begin, cur = 0;
+    while (base < b_end) {
+        const uint32_t span = min(kSpan, b_end - base);
+        if (io.loaded[cur] != base) {   // the first span, or the previous span stopped early
+            if (!io.drain(0) || !io.drain(1)) return false;
+            io.fetch(cur, base, span);
         }
         const uint32_t next = base + span;
-        if (next < nb) fetch(cur ^ 1, next, min(kSpan, nb - next));
-        if (!drain(cur)) { failed = true; break; }
-        const Summ* rec = reinterpret_cast<const Summ*>(sraw + cur * kSpanBuf + s_skew[cur]);
-        const double c = s_c;
+        if (next < b_end) io.fetch(cur ^ 1, next, min(kSpan, b_end - next));
+        if (!io.drain(cur)) return false;
+        const Summ* rec = io.rec(cur);
+        const double c = S.c;
         const int e0 = epoch_of(c);
         const uint32_t p0 = t * kChainPer;           // this thread's first position in the span
         uint64_t d0[kChainPer], d1[kChainPer];
@@ -930,11 +937,11 @@ __global__ void __launch_bounds__(kBT, 1) k_cdf_chain(const double* __restrict__
             const uint32_t pos = p0 + k;
             if (pos < span && !summ_pick(rec[pos], e0, d0[k], d1[k]) && my_bad == span) my_bad = pos;
         }
-        if (t == 0) s_end = span;
+        if (t == 0) S.end = span;
         __syncthreads();
-        if (my_bad < span) atomicMin(&s_end, my_bad);
+        if (my_bad < span) atomicMin(&S.end, my_bad);
         __syncthreads();
-        const uint32_t bad = s_end;
+        const uint32_t bad = S.end;
         uint64_t m0 = 0, m1 = 0;
 #pragma unroll
         for (int k = 0; k < kChainPer; ++k) {
@@ -946,10 +953,10 @@ __global__ void __launch_bounds__(kBT, 1) k_cdf_chain(const double* __restrict__
         }
         uint64_t ex0, ex1;
         if (__syncthreads_and(m0 == m1)) {
-            block_scan_add(m0, ex0, sh);    // translations only: the prefix is a sum
+            block_scan_add(m0, ex0, S.sh);    // translations only: the prefix is a sum
             ex1 = ex0;
         } else {
-            block_scan_maps(m0, m1, ex0, ex1, sh);
+            block_scan_maps(m0, m1, ex0, ex1, S.sh);
         }
         const uint64_t C = c > 0.0 ? uint64_t(ldexp(c, 52 - e0)) : 0;
         uint64_t x = C + ((C & 1) ? ex1 : ex0);
@@ -961,19 +968,19 @@ __global__ void __launch_bounds__(kBT, 1) k_cdf_chain(const double* __restrict__
             x += (x & 1) ? d1[k] : d0[k];
             if (x >= kTwo53 && my_over == bad && p0 + k < bad) my_over = p0 + k;   // the sum leaves the binade here
         }
-        if (t == 0) s_end = bad;
+        if (t == 0) S.end = bad;
         __syncthreads();
-        if (my_over < bad) atomicMin(&s_end, my_over);
+        if (my_over < bad) atomicMin(&S.end, my_over);
         __syncthreads();
-        const uint32_t end = s_end;
+        const uint32_t end = S.end;
 #pragma unroll
         for (int k = 0; k < kChainPer; ++k) {
             const uint32_t pos = p0 + k;
             if (pos < end) cin[base + pos] = ldexp(double(xin[k]), e0 - 52);
-            if (pos + 1 == end) s_c = ldexp(double(xin[k] + ((xin[k] & 1) ? d1[k] : d0[k])), e0 - 52);
+            if (pos + 1 == end) S.c = ldexp(double(xin[k] + ((xin[k] & 1) ? d1[k] : d0[k])), e0 - 52);
         }
         if (t == 0 && end > 0) ++n_span;
-        __syncthreads();   // every thread is done with rec and s_c before either changes
+        __syncthreads();   // every thread is done with rec and S.c before either changes
         if (end >= span) {
             base = next;
             cur ^= 1;   // loaded[cur] == next: fetched above
@@ -983,7 +990,7 @@ __global__ void __launch_bounds__(kBT, 1) k_cdf_chain(const double* __restrict__
         ++n_single;
         const uint32_t b = base + end;
         if (t == 0) {
-            double cc = s_c;
+            double cc = S.c;
             cin[b] = cc;
             const int eb = epoch_of(cc);
             uint64_t b0, b1;
@@ -992,36 +999,168 @@ __global__ void __launch_bounds__(kBT, 1) k_cdf_chain(const double* __restrict__
                 uint64_t Cb = cc > 0.0 ? uint64_t(ldexp(cc, 52 - eb)) : 0;
                 uint64_t Co = Cb + ((Cb & 1) ? b1 : b0);
                 if (Co < kTwo53 && Co >= Cb) {
-                    s_c = ldexp(double(Co), eb - 52);
+                    S.c = ldexp(double(Co), eb - 52);
                     slow = 0;
                 }
             }
-            s_slow = slow;
+            S.slow = slow;
         }
         __syncthreads();
-        if (s_slow) {
+        if (S.slow) {
             ++n_exact;
             double p[kEPT];
-            load_block_prob(prob, uint64_t(b) * kBS, p, stage);
-            double cc = block_exact(kBS, s_c, nullptr, sh, stage);
-            if (t == 0) s_c = cc;
+            load_block_prob(prob, uint64_t(b) * kBS, p, S.stage);
+            double cc = block_exact(kBS, S.c, nullptr, S.sh, S.stage);
+            if (t == 0) S.c = cc;
         }
         __syncthreads();
         base = b + 1;
     }
+    return true;
+}
+
+// hand-off between consecutive segments of the chain: the exact sum after a
+// segment, valid once flag is 1
+struct ChainLink {
+    double value;
+    uint32_t flag;
+    uint32_t pad;
+};
+// polls of the wait for the previous segment's sum (with a short sleep each)
+constexpr uint32_t kLinkWaitLimit = 1u << 24;
+
+// The chain in segments of kSpan blocks, one CTA each, taken in order through
+// a ticket (so a segment's predecessor always runs earlier or at the same
+// time).  Ahead of knowing its exact incoming sum, a CTA composes its
+// segment's folds on the one or two binades its first block's guess allows.
+// When the predecessor publishes the exact sum before the segment (link[j -
+// 1]), the CTA applies the composed fold of that sum's binade if the whole
+// segment stays in it and publishes the sum after the segment at once, so
+// the hand-off along the segments costs one fold application each; only
+// segments where the sum changes binade (a few dozen in a 2^30-element
+// vector) pass their sum on after the sequential range routine.  Every CTA
+// then writes its segment's exact block starts with chain_range from the
+// exact incoming sum.  Waits are bounded: a CTA that gives up writes 4 to
+// *status and publishes nothing, so the ones after it give up too.
+// stats (zeroed before the launch): spans, single blocks, exact blocks, blocks.
+__global__ void __launch_bounds__(kBT, 1) k_cdf_chain(const double* __restrict__ prob,
+                                                   const Summ* __restrict__ summ, uint32_t nb, double* __restrict__ cin,
+                                                   uint32_t* __restrict__ stats, unsigned* __restrict__ status,
+                                                   ChainLink* __restrict__ link, uint32_t* __restrict__ ticket)
+{
+    extern __shared__ __align__(16) char sraw[];
+    __shared__ ChainShm S;
+    __shared__ uint32_t s_seg;
+    __shared__ uint64_t s_map[2][2];
+    __shared__ int s_mapok[2];
+    __shared__ int s_done;
+    __shared__ int s_fail;
+    const uint32_t t = threadIdx.x;
+    if (t == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.bar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.bar[1])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_seg = atomicAdd(ticket, 1u);
+        s_done = 0;
+        s_fail = 0;
+    }
+    __syncthreads();
+    const uint32_t j = s_seg;
+    const uint32_t b0 = j * kSpan, b1 = min(nb, b0 + kSpan), cnt = b1 - b0;
+    ChainIO io(S, sraw, summ);
+    uint32_t n_span = 0, n_single = 0, n_exact = 0;
+    io.fetch(0, b0, cnt);
+    bool ok = io.drain(0);
+    if (ok && j > 0) {
+        // the segment's fold on each binade its first block may start in
+        const Summ* rec = io.rec(0);
+        const int32_t eg = rec[0].e;
+        for (int kb = 0; kb < 2; ++kb) {
+            const int e = eg + kb;
+            const uint32_t p0 = t * kChainPer;
+            bool valid = eg != INT32_MIN;
+            uint64_t m0 = 0, m1 = 0;
+#pragma unroll
+            for (int k = 0; k < kChainPer; ++k) {
+                uint64_t d0 = 0, d1 = 0;
+                if (p0 + k < cnt && !summ_pick(rec[p0 + k], e, d0, d1)) valid = false;
+                uint64_t r0, r1;
+                compose(m0, m1, d0, d1, r0, r1);
+                m0 = r0;
+                m1 = r1;
+            }
+            // each thread's fold below 2^53 keeps the block total below 2^61 (no wrap)
+            valid = valid && m0 < kTwo53 && m1 < kTwo53;
+            if (!__syncthreads_and(valid)) {
+                if (t == 0) s_mapok[kb] = 0;
+                continue;
+            }
+            uint64_t ex0, ex1;
+            block_scan_maps(m0, m1, ex0, ex1, S.sh);
+            if (t == kBT - 1) {
+                uint64_t r0, r1;
+                compose(ex0, ex1, m0, m1, r0, r1);
+                s_map[kb][0] = r0;
+                s_map[kb][1] = r1;
+                s_mapok[kb] = 1;
+            }
+        }
+        __syncthreads();   // s_map / s_mapok written above
+        // the exact sum before the segment, then at once the one after it if
+        // the segment's fold on that sum's binade applies
+        if (t == 0) {
+            volatile uint32_t* f = &link[j - 1].flag;
+            uint32_t i = 0;
+            while (*f == 0u && i < kLinkWaitLimit) {
+                __nanosleep(64);
+                ++i;
+            }
+            if (*f == 0u) {
+                s_fail = 1;
+            } else {
+                __threadfence();
+                const double c = *(volatile double*)&link[j - 1].value;
+                S.c = c;
+                const int e = epoch_of(c);
+                const int kb = e - eg;
+                if (eg != INT32_MIN && (kb == 0 || kb == 1) && s_mapok[kb]) {
+                    const uint64_t C = c > 0.0 ? uint64_t(ldexp(c, 52 - e)) : 0;
+                    const uint64_t x = C + ((C & 1) ? s_map[kb][1] : s_map[kb][0]);
+                    if (x < kTwo53) {
+                        link[j].value = ldexp(double(x), e - 52);
+                        __threadfence();
+                        *(volatile uint32_t*)&link[j].flag = 1u;
+                        s_done = 1;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        ok = !s_fail;
+    } else if (t == 0) {
+        S.c = 0.0;
+    }
+    __syncthreads();
+    // the segment's own block starts from the exact incoming sum
+    if (ok) ok = chain_range(io, prob, b0, b1, cin, n_span, n_single, n_exact);
+    if (ok && t == 0 && !s_done) {
+        link[j].value = S.c;
+        __threadfence();
+        *(volatile uint32_t*)&link[j].flag = 1u;
+    }
     // no copy may still be writing shared memory when the CTA leaves
-    const bool d0 = drain(0), d1 = drain(1), drained = d0 && d1;
-    if (failed || !drained) {
+    const bool dr0 = io.drain(0), dr1 = io.drain(1);
+    if (!ok || !dr0 || !dr1) {
         if (t == 0) *(volatile unsigned*)status = 4u;
         return;
     }
     if (t == 0) {
-        cin[nb] = s_c;
+        if (b1 == nb) cin[nb] = S.c;
         if (stats) {
-            stats[0] = n_span;
-            stats[1] = n_single;
-            stats[2] = n_exact;
-            stats[3] = nb;
+            atomicAdd(stats + 0, n_span);
+            atomicAdd(stats + 1, n_single);
+            atomicAdd(stats + 2, n_exact);
+            if (j == 0) stats[3] = nb;
         }
     }
 }
@@ -1425,7 +1564,9 @@ CdfView build_cdf(qse_state* st)
         v.cin = bsum + nb;
         size_t off_summ = (size_t(nb) * 4 + 15) & ~size_t(15);
         size_t off_gtot = off_summ + size_t(nb) * sizeof(Summ);
-        ctx->scratch2.reserve(off_gtot + (size_t(nb) / kGT + 1) * 8 + kSummSlack);
+        size_t off_link = (off_gtot + (size_t(nb) / kGT + 1) * 8 + 15) & ~size_t(15);
+        size_t off_ticket = off_link + size_t((nb + kSpan - 1) / kSpan) * sizeof(ChainLink);
+        ctx->scratch2.reserve(off_ticket + 16 + kSummSlack);
         char* base = static_cast<char*>(ctx->scratch2.ptr);
         int32_t* guess = reinterpret_cast<int32_t*>(base);
         Summ* summ = reinterpret_cast<Summ*>(base + off_summ);
@@ -1449,12 +1590,18 @@ CdfView build_cdf(qse_state* st)
             count_launch(ctx);
         }
         const uint32_t ng = (nb + kGT - 1) / kGT;
+        const uint32_t nseg = (nb + kSpan - 1) / kSpan;
         k_guess_part<<<ng, kGT, 0, ctx->stream>>>(bsum, nb, gtot);
         k_guess_fin<<<ng, kGT, 0, ctx->stream>>>(bsum, nb, gtot, guess);
         k_cdf_summ<<<nb, kBT, 0, ctx->stream>>>(v.cdf, guess, summ);
+        ChainLink* link = reinterpret_cast<ChainLink*>(base + off_link);
+        uint32_t* ticket = reinterpret_cast<uint32_t*>(base + off_ticket);
+        uint32_t* stats = reinterpret_cast<uint32_t*>(v.cin + nb + 1);
+        QSE_CUDA(cudaMemsetAsync(link, 0, off_ticket + 16 - off_link, ctx->stream));
+        QSE_CUDA(cudaMemsetAsync(stats, 0, 16, ctx->stream));
         QSE_CUDA(cudaFuncSetAttribute(k_cdf_chain, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kChainSmem)));
-        k_cdf_chain<<<1, kBT, kChainSmem, ctx->stream>>>(v.cdf, summ, nb, v.cin,
-                                                        reinterpret_cast<uint32_t*>(v.cin + nb + 1), ctx->status_dev);
+        k_cdf_chain<<<nseg, kBT, kChainSmem, ctx->stream>>>(v.cdf, summ, nb, v.cin, stats, ctx->status_dev, link,
+                                                           ticket);
         QSE_CUDA(cudaGetLastError());
         count_launch(ctx, 4);
         // the array keeps the probabilities: shots rebuild the cumulative values
