@@ -858,9 +858,8 @@ double adjoint(qse_state* st, const qse_op* ops, size_t nops, const double* para
 {
     qse_ctx* ctx = st->ctx;
     if (st->n < 3) fail(QSE_ERR_SIZE, "adjoint needs at least 3 qubits");
-    // forward from |0..0>
-    launch_init_zero_state(st);
-    for (uint32_t q = 0; q < st->n; ++q) st->perm[q] = q;
+    // forward from |0..0> (recorded: the first pass generates it)
+    mark_zero(st);
     execute_program(st, ops, nops, params, nparams, nullptr, nullptr, 0, nullptr);
     if (!st->aux) QSE_CUDA(cudaMalloc(&st->aux, st->size() * 16));
     double value = run_obs(st, obs, reinterpret_cast<double2*>(st->aux));
@@ -873,20 +872,47 @@ double adjoint(qse_state* st, const qse_op* ops, size_t nops, const double* para
     rev.reserve(nops);
     std::map<std::pair<int32_t, double>, int32_t> bucket_of;
     std::vector<std::pair<int32_t, double>> buckets;
+    // bucket of an occurrence of `param` whose angle moves by dtheta per unit
+    // of the parameter, on a gate of the given type
+    auto bucket = [&](int type, int32_t param, double dtheta) {
+        const double f = (type == QSE_GATE_PHASE || type == QSE_GATE_CPHASE || type == QSE_GATE_MCPHASE) ? -2.0 : 1.0;
+        const std::pair<int32_t, double> key{param, dtheta * f};
+        auto it = bucket_of.find(key);
+        if (it == bucket_of.end()) {
+            it = bucket_of.emplace(key, int32_t(buckets.size())).first;
+            buckets.push_back(key);
+        }
+        return it->second;
+    };
     for (size_t i = nops; i-- > 0;) {
+        // CNOT(c,t) RZ(th,t) CNOT(c,t) = exp(-i th/2 Z_c Z_t) = RZ(th,c) PHASE(th,t)
+        // CPHASE(-2th,c,t), exactly (global phase included): the reverse sweep
+        // undoes the three commuting phase gates, each an occurrence of the
+        // RZ's parameter (angle derivatives coeff, coeff, -2 coeff), instead of
+        // two CNOTs that each need their target in registers
+        if (i >= 2 && ops[i].type == QSE_GATE_CNOT && ops[i - 1].type == QSE_GATE_RZ &&
+            ops[i - 2].type == QSE_GATE_CNOT && ops[i].control == ops[i - 2].control &&
+            ops[i].target == ops[i - 2].target && ops[i - 1].target == ops[i].target &&
+            ops[i].control != ops[i].target) {
+            const qse_op& rz = ops[i - 1];
+            const double th = bound_angle(rz, params, nparams);
+            const bool p = rz.param >= 0;
+            qse_op a = rz;
+            a.target = ops[i].control;
+            qse_op b = rz;
+            b.type = QSE_GATE_PHASE;
+            qse_op c = rz;
+            c.type = QSE_GATE_CPHASE;
+            c.control = ops[i].control;
+            rev.push_back(inverse_gate(a, th, p ? bucket(QSE_GATE_RZ, rz.param, rz.coeff) : -1));
+            rev.push_back(inverse_gate(b, th, p ? bucket(QSE_GATE_PHASE, rz.param, rz.coeff) : -1));
+            rev.push_back(inverse_gate(c, -2.0 * th, p ? bucket(QSE_GATE_CPHASE, rz.param, -2.0 * rz.coeff) : -1));
+            i -= 2;
+            continue;
+        }
         double th = bound_angle(ops[i], params, nparams);
         int32_t gid = -1;
-        if (ops[i].param >= 0 && parameterised(ops[i].type)) {
-            const double f = (ops[i].type == QSE_GATE_PHASE || ops[i].type == QSE_GATE_CPHASE ||
-                              ops[i].type == QSE_GATE_MCPHASE) ? -2.0 : 1.0;
-            const std::pair<int32_t, double> key{ops[i].param, ops[i].coeff * f};
-            auto it = bucket_of.find(key);
-            if (it == bucket_of.end()) {
-                it = bucket_of.emplace(key, int32_t(buckets.size())).first;
-                buckets.push_back(key);
-            }
-            gid = it->second;
-        }
+        if (ops[i].param >= 0 && parameterised(ops[i].type)) gid = bucket(ops[i].type, ops[i].param, ops[i].coeff);
         rev.push_back(inverse_gate(ops[i], th, gid));
     }
     plan::Options opt;

@@ -114,6 +114,7 @@ struct Gen {
     std::string SYNC = "__syncthreads();";   // barrier of the threads that share xb
     // gradient slots accumulated per thread (slot -> accumulator index)
     static constexpr uint32_t kRegSlots = 4;
+    bool qv = false;   // qz holds Im(conj(l) s) of the registers as they are
     std::map<uint16_t, uint32_t> gacc;
     // the per-CTA group values come precomputed from global memory (gvt, one row
     // of ng values per tile): the prologue copies them instead of summing terms
@@ -264,9 +265,32 @@ struct Gen {
     {
         if (P.acc_mul) {
             if (diag_kind(op.kind)) { run_ops.push_back(op); return; }
+            // A phase generator's gradient sums sign * Im(conj(l) s) per
+            // amplitude, which the diagonal phases still pending for both
+            // states leave unchanged (unless a pending constant is not of unit
+            // modulus): it is taken without applying them, from one cached
+            // Im(conj(l) s) per register shared by every such occurrence of the
+            // run, and the run of phases stays open.
+            if (ns == 2 && (op.kind == plan::K_GRAD_Z || op.kind == plan::K_GRAD_P) && run_unimodular()) {
+                if (!qv) {
+                    for (uint32_t j = 0; j < R; ++j) o << "  qz[" << j << "] = im_ls(a1[" << j << "], a0[" << j << "]);";
+                    o << "\n";
+                    qv = true;
+                }
+                emit_grad(op, true);
+                return;
+            }
             flush_run();
         }
         emit(op);
+    }
+
+    // no pending constant of the open run scales the amplitudes
+    bool run_unimodular() const
+    {
+        for (const plan::KOp& k : run_ops)
+            if (k.kind == plan::K_FLUSH_ALL && std::fabs(k.a * k.a + k.b * k.b - 1.0) > 1e-12) return false;
+        return true;
     }
 
     static std::string cond_t(const char* v, uint16_t tc)
@@ -352,6 +376,7 @@ struct Gen {
         for (auto it = fac.begin(); it != fac.end();)
             it = (it->second.items.empty() && !it->second.hc) ? fac.erase(it) : std::next(it);
         if (fac.empty()) return;
+        qv = false;   // the phases change the registers
         o << "  {\n";
         std::vector<int> masks;
         std::map<int, std::string> val;
@@ -439,6 +464,7 @@ struct Gen {
         std::swap(o, head);
         o << "  const u32 tid = threadIdx.x;\n";
         for (const auto& kv : gacc) o << "  double gs" << kv.second << " = 0.0;\n";
+        if (ns == 2) o << "  double qz[" << R << "]; (void)qz;\n";
         o << "  extern __shared__ double2 sm[];\n";
         o << "  double2* xb = sm; (void)xb;\n";
         o << "  double2* gv = sm + " << tsize << "; (void)gv;\n";
@@ -856,6 +882,7 @@ struct Gen {
     void emit(const plan::KOp& op)
     {
         using namespace plan;
+        if (op.kind < K_GRAD_X || op.kind > K_GRAD_P) qv = false;   // the registers may change
         const int p = op.p;
         const std::string c = cond(op.tcond, op.ocond);
         auto guarded = [&](const std::string& stmt) {
@@ -946,19 +973,33 @@ struct Gen {
             o << "    gb = " << gbase_expr() << ";\n  }\n";
             break;
         }
-        case K_GRAD_X: case K_GRAD_Y: case K_GRAD_Z: case K_GRAD_P: {
-            if (ns != 2) break;
+        case K_GRAD_X: case K_GRAD_Y: case K_GRAD_Z: case K_GRAD_P: emit_grad(op, false); break;
+        default: break;
+        }
+    }
+
+    // One gradient occurrence.  cached: phase generators read the per-register
+    // Im(conj(l) s) in qz (taken while diagonal phases are still pending).
+    void emit_grad(const plan::KOp& op, bool cached)
+    {
+        using namespace plan;
+        if (ns != 2) return;
+        const int p = op.p;
+        const std::string c = cond(op.tcond, op.ocond);
+        {
             std::string expr;
             if (op.kind == K_GRAD_X) expr = "gradX<" + std::to_string(p) + ">(a0, a1)";
             else if (op.kind == K_GRAD_Y) expr = "gradY<" + std::to_string(p) + ">(a0, a1)";
             else if (op.kind == K_GRAD_Z) {
-                expr = "gradZ<" + std::to_string(p < int(P.rb) ? p : -1) + ">(a0, a1)";
+                expr = std::string(cached ? "gradZq<" : "gradZ<") + std::to_string(p < int(P.rb) ? p : -1) +
+                       (cached ? ">(qz)" : ">(a0, a1)");
                 std::string sg;
                 if (op.tcond) sg += "((tid & " + std::to_string(op.tcond) + "u) != 0u)";
                 if (op.ocond) sg += std::string(sg.empty() ? "" : " != ") + "((ob & " + hex(op.ocond) + ") != 0ull)";
                 if (!sg.empty()) expr = "((" + sg + ") ? -" + expr + " : " + expr + ")";
             } else {
-                expr = "gradP<" + std::to_string(int(op.f)) + ">(a0, a1)";
+                expr = std::string(cached ? "gradPq<" : "gradP<") + std::to_string(int(op.f)) +
+                       (cached ? ">(qz)" : ">(a0, a1)");
                 if (!c.empty()) expr = "((" + c + ") ? " + expr + " : 0.0)";
             }
             const uint32_t si = push(op.a);
@@ -972,9 +1013,6 @@ struct Gen {
             else
                 o << "  { const double v = warpSum<" << T << ">(" << expr << " * P.v[" << si << "]);"
                   << " if ((tid & 31u) == 0u) wp[" << op.g << "u * " << NW << "u + (tid >> 5)] += v; }\n";
-            break;
-        }
-        default: break;
         }
     }
 };
