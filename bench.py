@@ -89,6 +89,8 @@ def parse():
     ap.add_argument("--pass-kernel", type=int, default=-1, choices=[-1, 0, 1, 2],
                     help="pass kernels (qse_ctx_set_jit): 0 interpreter, 1 one CTA per tile, 2 streamed; "
                          "-1 = library default")
+    ap.add_argument("--adjoint", type=int, default=0, metavar="QUBITS",
+                    help="instead of the step: only the adjoint section (Max-Cut QAOA, p = 2) at QUBITS qubits")
     ap.add_argument("--sharded", type=int, default=0, metavar="QUBITS",
                     help="instead of the step: one H+RZ+QFT state of QUBITS qubits sharded over the N ranks "
                          "(2^g = N, the top g qubits global; NCCL half-shard exchanges), execute only")
@@ -459,6 +461,13 @@ def main():
     if args.playground:
         if rank == 0:
             print(json.dumps(bench_playground(Device(local), args.playground)))
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    if args.adjoint:
+        if rank == 0:
+            print(json.dumps(bench_adjoint_30q(Device(local), L, W, np, n=args.adjoint)))
         if dist:
             dist.destroy_process_group()
         return
@@ -859,26 +868,34 @@ def bench_qaoa(dev, L, W, np, plain=True):
     return out
 
 
-def bench_adjoint_30q(dev, L, W, np):
-    """Adjoint at 30 qubits on one GPU (two 16 GiB states): Max-Cut QAOA on a random
-    3-regular graph with 30 nodes, p = 2 (4 parameters).  Reports gradients/s and
-    the HBM fraction of the reverse passes (64 B per amplitude: psi and lambda read
-    and written, the <lambda|dG|psi> reductions fused)."""
+def bench_adjoint_30q(dev, L, W, np, n=30):
+    """Adjoint at n qubits (30 by default: two 16 GiB states on one GPU): Max-Cut QAOA
+    on a random 3-regular graph with n nodes, p = 2 (4 parameters).  Reports
+    gradients/s, the device time of every pass (forward, then reverse) and the HBM
+    fraction of the reverse passes (64 B per amplitude: psi and lambda read and
+    written, the <lambda|dG|psi> reductions fused)."""
     import torch
     from quantumsimevo_b200.circuit import StateVector
-    if torch.cuda.mem_get_info(dev.index)[0] < (40 << 30):
-        return {"skipped": "less than 40 GiB of free device memory"}
-    n, p = 30, 2
+    if torch.cuda.mem_get_info(dev.index)[0] < 40 * (1 << n):   # two states of 16 B per amplitude, and slack
+        return {"skipped": "not enough free device memory for two states"}
+    p = 2
     ops, params, edges, obs_t = W.qaoa_maxcut(n, p, seed=30)
     obs, keep = L.observable(*obs_t)
     st = StateVector(n, dev)
     pp = np.ascontiguousarray(params)
     g = np.zeros(pp.size)
     v = C.c_double()
-    stats = L.QseExecStats()
+    # timed forward passes of the same execute (passes on a compact state are not timed)
+    L.check(L.lib.qse_ctx_time_passes(dev.handle, 1))
+    fl = np.zeros(256)
+    fc = C.c_size_t()
+    L.check(L.lib.qse_ctx_pass_time_list(dev.handle, fl.ctypes.data_as(L._pd), fl.size, C.byref(fc)))
     L.check(L.lib.qse_execute(st.handle, L.dptr(ops), len(ops), pp.ctypes.data_as(L._pd), pp.size, None, None, 0,
-                              C.byref(stats)))
-    fwd = int(stats.passes)
+                              None))
+    dev.synchronize()
+    L.check(L.lib.qse_ctx_pass_time_list(dev.handle, fl.ctypes.data_as(L._pd), fl.size, C.byref(fc)))
+    L.check(L.lib.qse_ctx_time_passes(dev.handle, 0))
+    fwd = int(fc.value)
 
     def adjoint():
         L.check(L.lib.qse_adjoint(st.handle, L.dptr(ops), len(ops), pp.ctypes.data_as(L._pd), pp.size,
@@ -909,6 +926,7 @@ def bench_adjoint_30q(dev, L, W, np):
         "reverse_pass_ms": float(rev.mean()) if rev.size else None,
         "reverse_pass_gbs": rev_gbs,
         "reverse_pass_hbm_frac": rev_gbs / hbm_peak if rev_gbs else None,
+        "pass_ms": [round(float(x), 4) for x in plist],
         "peak_kind": peak_kind,
         "value": v.value,
         "timing": "CUDA events on the library stream around one qse_adjoint; pass times from per-launch events",
