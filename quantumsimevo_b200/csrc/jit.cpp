@@ -104,6 +104,22 @@ struct Gen {
     // physical qubit after this pass; empty = none (emit_prob)
     std::vector<uint8_t> lpos;
     bool prob_bsum = false;   // the side output includes the block sums
+    // debug mode (QSE_DEBUG_BOUNDS set in the environment when the kernel is
+    // generated): every global access of the kernel checks its index against
+    // the array's size; one outside records 8 in *status and is skipped
+    bool dbg = false;
+    std::string nstr() const { return hex(uint64_t(1) << (P.k + uint32_t(__builtin_popcountll(P.outer_mask)))); }
+    // array[idx] as an operand (a zero amplitude when out of range in debug mode)
+    std::string ld(const std::string& arr, const std::string& idx, const std::string& size) const
+    {
+        if (!dbg) return arr + "[" + idx + "]";
+        return "(qse_idx_ok(" + idx + ", " + size + ", status) ? " + arr + "[" + idx + "] : make_double2(0.0, 0.0))";
+    }
+    // prefix of a statement that writes at idx (skipped when out of range in debug mode)
+    std::string guard(const std::string& idx, const std::string& size) const
+    {
+        return dbg ? "if (qse_idx_ok(" + idx + ", " + size + ", status)) " : std::string();
+    }
     // kernel names tell the input kinds apart in profiles
     std::string kernel_name() const
     {
@@ -442,8 +458,9 @@ struct Gen {
         flush_run();
         // store (final layout)
         for (uint32_t j = 0; j < R; ++j) {
-            o << "  psi[gb + " << hex(reg_off(j)) << "] = a0[" << j << "];";
-            if (ns == 2) o << " lam[gb + " << hex(reg_off(j)) << "] = a1[" << j << "];";
+            const std::string ix = "gb + " + hex(reg_off(j));
+            o << "  " << guard(ix, nstr()) << "psi[" << ix << "] = a0[" << j << "];";
+            if (ns == 2) o << " " << guard(ix, nstr()) << "lam[" << ix << "] = a1[" << j << "];";
             o << "\n";
         }
         if (!lpos.empty()) emit_prob();
@@ -497,7 +514,8 @@ struct Gen {
                     const uint64_t m = uint64_t(j) * T;
                     for (uint32_t b = lt; b < P.k; ++b)
                         if ((m >> b) & 1) cj |= uint64_t(1) << P.tile_phys[b];
-                    o << "    psi[gz + " << hex(cj) << "] = make_double2(0.0, 0.0);\n";
+                    o << "    " << guard("gz + " + hex(cj), nstr()) << "psi[gz + " << hex(cj)
+                      << "] = make_double2(0.0, 0.0);\n";
                 }
                 o << "    return;\n  }\n";
             }
@@ -509,8 +527,9 @@ struct Gen {
         for (int s = 0; s < ns; ++s) o << "  double2 a" << s << "[" << R << "];\n";
         if (!zero_in) {
             for (uint32_t j = 0; j < R; ++j) {
-                o << "  a0[" << j << "] = psi[gb + " << hex(reg_off(j)) << "];";
-                if (ns == 2) o << " a1[" << j << "] = lam[gb + " << hex(reg_off(j)) << "];";
+                const std::string ix = "gb + " + hex(reg_off(j));
+                o << "  a0[" << j << "] = " << ld("psi", ix, nstr()) << ";";
+                if (ns == 2) o << " a1[" << j << "] = " << ld("lam", ix, nstr()) << ";";
                 o << "\n";
             }
         } else if (umask) {
@@ -541,14 +560,16 @@ struct Gen {
                     }
                 o << "  a0[" << j << "] = ";
                 if (tz) o << "((((gb | " << hex(reg_off(j)) << ") ^ bi) & " << hex(tz) << ") == 0ull) ? ";
-                o << "lam[cb + " << hex(coff) << "]";
+                o << ld("lam", "cb + " + hex(coff), hex(uint64_t(1) << __builtin_popcountll(umask)));
                 if (tz) o << " : make_double2(0.0, 0.0)";
                 o << ";\n";
             }
         }
         // prologue: per-CTA diagonal group values, then the lane tables
         if (ng && pre_gv) {
-            o << "  for (u32 g = tid; g < " << ng << "u; g += " << T << "u) gv[g] = gvt[(u64)blockIdx.x * " << ng << "u + g];\n";
+            o << "  for (u32 g = tid; g < " << ng << "u; g += " << T << "u) gv[g] = "
+              << ld("gvt", "(u64)blockIdx.x * " + std::to_string(ng) + "u + g", "(u64)gridDim.x * " + std::to_string(ng) + "u")
+              << ";\n";
         } else if (ng) {
             // the pass's terms are first copied into the exchange buffer (unused until
             // the first layout exchange, which follows the prologue's barrier) by every
@@ -668,8 +689,8 @@ struct Gen {
             uint64_t lk = 0;
             for (uint32_t i = lt; i < P.k; ++i)
                 if (((uint64_t(kk) * T) >> i) & 1) lk |= uint64_t(1) << lsorted[i];
-            o << "    const double p" << kk << " = pb[sw(tid + " << kk * T << "u)]; prob[lbt | " << hex(lk) << "] = p" << kk
-              << ";\n";
+            o << "    const double p" << kk << " = pb[sw(tid + " << kk * T << "u)]; "
+              << guard("lbt | " + hex(lk), hex(uint64_t(1) << n)) << "prob[lbt | " << hex(lk) << "] = p" << kk << ";\n";
             keys[lk >> 12].push_back(kk);
         }
         prob_bsum = i0 >= 5;
@@ -717,7 +738,8 @@ struct Gen {
             ki = 0;
             for (const auto& kv : keys) {
                 o << "    if (tid == " << ki << "u) { double v = 0.0; for (u32 w = 0; w < " << NW << "u; ++w) v += bs["
-                  << ki * NW << "u + w]; atomicAdd(bsum + ((lb >> 12) | " << hex(kv.first) << "), v); }\n";
+                  << ki * NW << "u + w]; " << guard("((lb >> 12) | " + hex(kv.first) + ")", hex(uint64_t(1) << n >> 12))
+                  << "atomicAdd(bsum + ((lb >> 12) | " << hex(kv.first) << "), v); }\n";
                 ++ki;
             }
         } else if (prob_bsum) {
@@ -726,8 +748,9 @@ struct Gen {
                 uint64_t lk = 0;
                 for (uint32_t i = lt; i < P.k; ++i)
                     if (((uint64_t(kk) * T) >> i) & 1) lk |= uint64_t(1) << lsorted[i];
-                o << "    { const double v = warpSum<" << T << ">(p" << kk << "); if ((tid & 31u) == 0u) atomicAdd(bsum + ((lbt | "
-                  << hex(lk) << ") >> 12), v); }\n";
+                const std::string bix = "((lbt | " + hex(lk) + ") >> 12)";
+                o << "    { const double v = warpSum<" << T << ">(p" << kk << "); if ((tid & 31u) == 0u) { "
+                  << guard(bix, hex(uint64_t(1) << n >> 12)) << "atomicAdd(bsum + " << bix << ", v); } }\n";
             }
         }
         // else: lane bits at logical positions >= 12 (a warp's 32 values span
@@ -1075,7 +1098,9 @@ static bool streamable(const plan::PassProgram& p, int nstates, bool basis_input
 Source generate(const plan::PassProgram& p, int nstates, bool basis_input, bool streamed, bool precomputed_groups,
                 uint64_t compact_mask, const uint8_t* prob_lpos)
 {
-    if (streamed && !prob_lpos && streamable(p, nstates, basis_input)) {
+    const char* dbg_env = std::getenv("QSE_DEBUG_BOUNDS");
+    const bool dbg = dbg_env && *dbg_env && std::strcmp(dbg_env, "0") != 0;
+    if (streamed && !dbg && !prob_lpos && streamable(p, nstates, basis_input)) {
         Gen g(p, nstates, false);
         Source s;
         s.code = g.run_streamed();
@@ -1088,6 +1113,7 @@ Source generate(const plan::PassProgram& p, int nstates, bool basis_input, bool 
         }
     }
     Gen g(p, nstates, basis_input, precomputed_groups, compact_mask);
+    g.dbg = dbg;
     // (not with a tile that stores zeros and returns early: a basis input with outer bits)
     if (prob_lpos && nstates == 1 && !(g.zero_in && (p.outer_mask & ~g.umask) != 0))
         g.lpos.assign(prob_lpos, prob_lpos + 64);

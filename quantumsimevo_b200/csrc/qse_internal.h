@@ -150,7 +150,8 @@ inline void check_device_status(qse_ctx* ctx)
     if (v == 0u) return;
     *s = 0u;
     fail(QSE_ERR_TIMEOUT, "a kernel's bounded wait gave up (status " + std::to_string(v) +
-                              ": 1-2 a streamed pass, 4 the sampling scan); its results are invalid");
+                              ": 1-2 a streamed pass, 4 the sampling scan, 8 a pass kernel's index check in "
+                              "QSE_DEBUG_BOUNDS mode); its results are invalid");
 }
 
 // ---- per-gate ("plain method") kernels: gates.cu ----
