@@ -110,7 +110,10 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 100 ms.  start()
+    returns once the first sample is written, so that sampling runs through the
+    whole timed region; stop() reads the samples written after start() returned
+    (the last earlier one when the region was shorter than the interval)."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -119,16 +122,22 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.proc = None
+        self.offset = 0
         self.path = os.path.join(tempfile.gettempdir(), f"qse_clocks_{os.getpid()}.csv")
 
     def start(self):
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        t0 = time.time()
+        while os.path.getsize(self.path) == 0 and time.time() - t0 < 5.0 and self.proc.poll() is None:
+            time.sleep(0.01)
+        self.offset = os.path.getsize(self.path)
 
     def stop(self):
         if self.proc is None:
@@ -142,23 +151,28 @@ class ClockSampler:
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         with open(self.path) as f:
-            for line in f:
-                p = [x.strip() for x in line.split(",")]
-                if len(p) < 9:
-                    continue
-                try:
-                    sm.append(float(p[1]))
-                    smax = float(p[2])
-                except ValueError:
-                    continue
-                for nm, v in zip(names, p[5:9]):
-                    if v.lower() == "active":
-                        reasons.add(nm)
+            text = f.read()
+        lines = text[self.offset:].splitlines()
+        in_region = len(lines)
+        if not lines:
+            lines = text[:self.offset].splitlines()[-1:]
+        for line in lines:
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
         os.unlink(self.path)
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "samples_in_region": in_region}
 
 
 # ---------------------------------------------------------------- reference code (oracle/_ref)

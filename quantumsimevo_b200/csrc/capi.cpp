@@ -171,6 +171,7 @@ int qse_ctx_destroy(qse_ctx* ctx)
     bind_device(ctx);
     cudaStreamSynchronize(ctx->stream);
     qse::destroy_compact_state(ctx);
+    qse::destroy_plan_cache(ctx);
     ctx->plan_buf.release();
     ctx->scratch.release();
     ctx->scratch2.release();

@@ -37,7 +37,92 @@ uint64_t physical_to_logical_index(const qse_state* st, uint64_t P)
     return L;
 }
 
+// ---- plan cache ----
+// An execute of a program that ran before on a state in the same layout (a
+// sampling loop that runs one circuit from |0..0> again and again, a repeated
+// adjoint sweep at fixed parameters) reuses that plan: its pass programs, its
+// kernels' sources and the compiled kernels.  Planning a 500-gate circuit and
+// generating its kernels' sources takes close to a millisecond of host time,
+// during which the device has nothing queued.  An entry's key holds every input
+// the plan depends on, written field by field (plan::Gate has padding).
+struct PlanEntry {
+    std::string key;
+    size_t hash = 0;
+    uint64_t used = 0;
+    plan::Plan pl;
+    bool use_jit = false;
+    std::vector<jit::Source> srcs;
+    std::vector<std::shared_ptr<jit::Kernel>> ks;   // filled by the first run
+};
+
+struct PlanCache {
+    std::vector<std::shared_ptr<PlanEntry>> entries;
+    uint64_t tick = 0;
+};
+
+void destroy_plan_cache(qse_ctx* ctx)
+{
+    delete ctx->plan_cache;
+    ctx->plan_cache = nullptr;
+}
+
 namespace {
+
+constexpr size_t kPlanCacheEntries = 16;
+
+struct KeyWriter {
+    std::string s;
+    template <class T>
+    void put(const T& v)
+    {
+        s.append(reinterpret_cast<const char*>(&v), sizeof(T));
+    }
+    void put_options(const plan::Options& o)
+    {
+        put(o.k); put(o.rb); put(o.max_gates); put(o.max_terms); put(o.grads); put(o.max_slots);
+        put(o.direct_phases); put(o.acc_mul); put(o.zz_fuse); put(o.keep_gphase);
+    }
+    void put_gates(const std::vector<plan::Gate>& gates)
+    {
+        put(uint64_t(gates.size()));
+        s.reserve(s.size() + gates.size() * 96);
+        for (const plan::Gate& g : gates) {
+            put(g.type); put(g.t); put(g.c); put(g.cmask); put(g.theta); put(g.grad);
+            s.append(reinterpret_cast<const char*>(g.m), sizeof g.m);
+        }
+    }
+    // the state's layout: qubit count and logical -> physical map
+    void put_state(const qse_state* st)
+    {
+        put(st->n);
+        s.append(reinterpret_cast<const char*>(st->perm), st->n * sizeof(uint32_t));
+    }
+};
+
+std::shared_ptr<PlanEntry> plan_cache_find(qse_ctx* ctx, const std::string& key, size_t hash)
+{
+    if (!ctx->plan_cache) return nullptr;
+    for (auto& e : ctx->plan_cache->entries)
+        if (e->hash == hash && e->key == key) {
+            e->used = ++ctx->plan_cache->tick;
+            return e;
+        }
+    return nullptr;
+}
+
+void plan_cache_insert(qse_ctx* ctx, std::shared_ptr<PlanEntry> e)
+{
+    if (!ctx->plan_cache) ctx->plan_cache = new PlanCache;
+    PlanCache& c = *ctx->plan_cache;
+    e->used = ++c.tick;
+    if (c.entries.size() < kPlanCacheEntries) {
+        c.entries.push_back(std::move(e));
+        return;
+    }
+    auto lru = std::min_element(c.entries.begin(), c.entries.end(),
+                                [](const auto& a, const auto& b) { return a->used < b->used; });
+    *lru = std::move(e);   // an entry still in use by a caller stays alive through its shared_ptr
+}
 
 plan::Gate to_gate(const qse_op& op, double theta)
 {
@@ -243,29 +328,55 @@ constexpr size_t kJitMaxNewKernels = 32;
 // Plans gates for the specialised kernels (their sources generated into srcs,
 // use_jit = true) or, when the context disables them or they are not worth
 // compiling, for the interpreter (angle accumulators, use_jit = false).
-plan::Plan plan_for(qse_state* st, const std::vector<plan::Gate>& gates, plan::Options opt, int ns, bool& use_jit,
-                    std::vector<jit::Source>& srcs, bool prob_out = false)
+// Specialised plans are kept in the context's plan cache.
+std::shared_ptr<PlanEntry> plan_for(qse_state* st, const std::vector<plan::Gate>& gates, plan::Options opt, int ns,
+                                    bool prob_out = false)
 {
-    use_jit = st->ctx->jit != 0;
-    opt.acc_mul = use_jit;
-    plan::Plan pl = plan::build(gates, st->n, st->perm, opt);
-    srcs.clear();
-    if (!use_jit) return pl;
-    srcs.reserve(pl.passes.size());
+    qse_ctx* ctx = st->ctx;
+    auto e = std::make_shared<PlanEntry>();
+    e->use_jit = ctx->jit != 0;
+    opt.acc_mul = e->use_jit;
+    if (e->use_jit) {
+        KeyWriter w;
+        w.put('F');
+        w.put(ctx->jit);
+        w.put(ns);
+        w.put(prob_out);
+        w.put(st->lazy_basis);
+        w.put(st->lazy_basis ? st->lazy_umask : 0);
+        const char* dbg = std::getenv("QSE_DEBUG_BOUNDS");   // read by jit::generate
+        w.s.append(dbg ? dbg : "");
+        w.put('\0');
+        w.put_options(opt);
+        w.put_state(st);
+        w.put_gates(gates);
+        e->key = std::move(w.s);
+        e->hash = std::hash<std::string>{}(e->key);
+        if (auto hit = plan_cache_find(ctx, e->key, e->hash)) return hit;
+    }
+    e->pl = plan::build(gates, st->n, st->perm, opt);
+    if (!e->use_jit) return e;
+    const plan::Plan& pl = e->pl;
+    e->srcs.reserve(pl.passes.size());
     // the last pass may also write the probabilities in logical order
     uint8_t lpos[64] = {0};
     for (uint32_t q = 0; q < st->n; ++q) lpos[pl.perm_final[q]] = uint8_t(q);
     for (size_t i = 0; i < pl.passes.size(); ++i) {
         const bool basis_in = i == 0 && ns == 1 && st->lazy_basis;
         const bool prob = prob_out && ns == 1 && i + 1 == pl.passes.size();
-        srcs.push_back(jit::generate(pl.passes[i], ns, basis_in, st->ctx->jit == 2, st->n >= jit::kPreGroupQubits,
-                                     basis_in ? st->lazy_umask : 0, prob ? lpos : nullptr));
+        e->srcs.push_back(jit::generate(pl.passes[i], ns, basis_in, ctx->jit == 2, st->n >= jit::kPreGroupQubits,
+                                        basis_in ? st->lazy_umask : 0, prob ? lpos : nullptr));
     }
-    if (st->n >= kJitAlwaysQubits || jit::count_uncached(srcs) <= kJitMaxNewKernels) return pl;
-    use_jit = false;
-    srcs.clear();
+    if (st->n >= kJitAlwaysQubits || jit::count_uncached(e->srcs) <= kJitMaxNewKernels) {
+        plan_cache_insert(ctx, e);
+        return e;
+    }
+    e->use_jit = false;
+    e->srcs.clear();
+    e->key.clear();
     opt.acc_mul = false;
-    return plan::build(gates, st->n, st->perm, opt);
+    e->pl = plan::build(gates, st->n, st->perm, opt);
+    return e;
 }
 
 // Runs the passes of a plan: specialised NVRTC kernels (jit.cpp, sources from
@@ -277,19 +388,18 @@ struct PassRunner {
     int ns;
     uint32_t rb;
     bool jit;
-    std::vector<jit::Source> srcs;
-    std::vector<std::shared_ptr<jit::Kernel>> ks;
+    const std::vector<jit::Source>& srcs;
+    const std::vector<std::shared_ptr<jit::Kernel>>& ks;
     std::vector<uint32_t> kq;
 
-    PassRunner(qse_state* s, const plan::Plan& pl, Uploaded& u, int nstates, uint32_t regbits, bool use_jit,
-               std::vector<jit::Source>&& sources)
-        : ctx(s->ctx), st(s), up(u), ns(nstates), rb(regbits), jit(use_jit), srcs(std::move(sources))
+    PassRunner(qse_state* s, PlanEntry& e, Uploaded& u, int nstates, uint32_t regbits)
+        : ctx(s->ctx), st(s), up(u), ns(nstates), rb(regbits), jit(e.use_jit), srcs(e.srcs), ks(e.ks)
     {
-        for (const auto& p : pl.passes) kq.push_back(p.k);
-        if (!jit) return;
+        for (const auto& p : e.pl.passes) kq.push_back(p.k);
+        if (!jit || e.ks.size() == e.srcs.size()) return;
         std::vector<const jit::Source*> ptrs;
-        for (const auto& s2 : srcs) ptrs.push_back(&s2);
-        ks = jit::get_kernels(ptrs);
+        for (const auto& s2 : e.srcs) ptrs.push_back(&s2);
+        e.ks = jit::get_kernels(ptrs);
     }
 
     void run(size_t i, double2* lam, double* part)
@@ -397,10 +507,11 @@ plan::Options fused_options(const qse_ctx* ctx, uint32_t n)
 uint64_t run_fused(qse_state* st, const std::vector<plan::Gate>& gates, bool prob_out = false)
 {
     qse_ctx* ctx = st->ctx;
-    bool use_jit = false;
-    std::vector<jit::Source> srcs;
     prob_out = prob_out && st->size() >= 4096 && ctx->jit != 0;
-    plan::Plan pl = plan_for(st, gates, fused_options(ctx, st->n), 1, use_jit, srcs, prob_out);
+    const std::shared_ptr<PlanEntry> e = plan_for(st, gates, fused_options(ctx, st->n), 1, prob_out);
+    const plan::Plan& pl = e->pl;
+    const bool use_jit = e->use_jit;
+    const std::vector<jit::Source>& srcs = e->srcs;
     if (!use_jit) materialize(st);  // interpreter passes read the state
     double* prob = nullptr;
     const bool with_bsum = !srcs.empty() && srcs.back().prob_bsum;
@@ -411,7 +522,7 @@ uint64_t run_fused(qse_state* st, const std::vector<plan::Gate>& gates, bool pro
         st->cdf_version = ~uint64_t(0);   // the buffer's cumulative values are overwritten
     }
     Uploaded up = upload_plan(ctx, pl, use_jit && st->n >= jit::kPreGroupQubits);
-    PassRunner runner(st, pl, up, 1, 4, use_jit, std::move(srcs));
+    PassRunner runner(st, *e, up, 1, 4);
     for (size_t i = 0; i < up.args.size(); ++i) runner.run(i, nullptr, i + 1 == up.args.size() ? prob : nullptr);
     if (!up.args.empty()) {   // the first pass wrote every amplitude
         st->lazy_basis = false;
@@ -556,7 +667,21 @@ bool compact_prefix(qse_state* st, const std::vector<plan::Gate>& gates_in, std:
     const std::vector<plan::Gate>& gates = plan::fuse_zz(gates_in, fused) ? fused : gates_in;
     opt.zz_fuse = false;
     opt.acc_mul = true;
-    const plan::Plan pl = plan::build(gates, st->n, st->perm, opt);
+    KeyWriter w;
+    w.put('C');
+    w.put_options(opt);
+    w.put_state(st);
+    w.put_gates(gates);
+    const size_t hash = std::hash<std::string>{}(w.s);
+    std::shared_ptr<PlanEntry> e = plan_cache_find(ctx, w.s, hash);
+    if (!e) {
+        e = std::make_shared<PlanEntry>();
+        e->pl = plan::build(gates, st->n, st->perm, opt);
+        e->key = std::move(w.s);
+        e->hash = hash;
+        plan_cache_insert(ctx, e);
+    }
+    const plan::Plan& pl = e->pl;
     size_t K = 0;
     uint64_t u = 0, uK = 0;
     for (size_t i = 0; i < pl.passes.size(); ++i) {
@@ -921,10 +1046,9 @@ double adjoint(qse_state* st, const qse_op* ops, size_t nops, const double* para
     opt.grads = true;
     opt.max_terms = 512;
     opt.max_gates = plan::kJitMaxGates;
-    bool use_jit = false;
-    std::vector<jit::Source> srcs;
-    plan::Plan pl = plan_for(st, rev, opt, 2, use_jit, srcs);
-    Uploaded up = upload_plan(ctx, pl, use_jit && st->n >= jit::kPreGroupQubits);
+    const std::shared_ptr<PlanEntry> e = plan_for(st, rev, opt, 2);
+    const plan::Plan& pl = e->pl;
+    Uploaded up = upload_plan(ctx, pl, e->use_jit && st->n >= jit::kPreGroupQubits);
 
     // occurrence gradients accumulate in scratch2: [nops] | slot partials
     size_t max_part = 0;
@@ -948,7 +1072,7 @@ double adjoint(qse_state* st, const qse_op* ops, size_t nops, const double* para
             std::memcpy(h + i * b_src, pl.passes[i].slot_src.data(), pl.passes[i].slot_src.size() * 4);
         QSE_CUDA(cudaMemcpyAsync(srcbase, h, b_src * pl.passes.size(), cudaMemcpyHostToDevice, ctx->stream));
     }
-    PassRunner runner(st, pl, up, 2, 3, use_jit, std::move(srcs));
+    PassRunner runner(st, *e, up, 2, 3);
     for (size_t i = 0; i < up.args.size(); ++i) {
         const tile::PassArgs& a = up.args[i];
         runner.run(i, reinterpret_cast<double2*>(st->aux), part);

@@ -35,6 +35,8 @@ struct DevBuf {
     ~DevBuf() { release(); }
 };
 
+struct PlanCache;   // engine.cu: plans of recent executes, reused when a program runs again
+
 // Pinned host staging buffer.
 struct HostBuf {
     void* ptr = nullptr;
@@ -81,6 +83,7 @@ struct qse_ctx {
     // leading passes of a circuit that leave the other qubits in their basis
     // state (engine.cu, compact_prefix); allocated on first use
     qse_state* compact = nullptr;
+    qse::PlanCache* plan_cache = nullptr;   // allocated on first use
 };
 
 struct qse_state {
@@ -174,6 +177,7 @@ void mark_zero(qse_state* st);       // reset without writing: lazy |0..0>
 int measure_or_reset_qubit(qse_state* st, uint32_t qubit, double u, bool reset, double* prob1);
 void materialize(qse_state* st);     // write a lazy basis (or compact) state into the array (no-op otherwise)
 void destroy_compact_state(qse_ctx* ctx);
+void destroy_plan_cache(qse_ctx* ctx);
 void launch_pauli_frame(qse_state* st, const int32_t* d_counts);      // Noise::applyPauliNoise
 void permute_to_logical(qse_state* st, double* dst_device);           // gather into logical order
 void scale_state(qse_state* st, double s);
