@@ -599,8 +599,8 @@ int qse_plan_compile(uint32_t nqubits, const qse_op* ops, size_t nops, const dou
     uint32_t perm[64];
     for (uint32_t q = 0; q < 64; ++q) perm[q] = q;
     qse::plan::Options opt;
-    opt.rb = nstates == 2 ? 3 : 4;
     opt.k = std::min<uint32_t>(tile_qubits ? tile_qubits : (nstates == 2 ? 11 : 12), nqubits);
+    opt.rb = nstates == 2 ? 3 : (!streamed && opt.k == 12) ? 5 : 4;   // as the engine plans them
     opt.grads = nstates == 2;
     opt.acc_mul = true;
     opt.max_gates = qse::plan::kJitMaxGates;

@@ -375,6 +375,7 @@ std::shared_ptr<PlanEntry> plan_for(qse_state* st, const std::vector<plan::Gate>
     e->srcs.clear();
     e->key.clear();
     opt.acc_mul = false;
+    opt.rb = std::min(opt.rb, 4u);   // the interpreter kernel holds at most 16 amplitudes per thread
     e->pl = plan::build(gates, st->n, st->perm, opt);
     return e;
 }
@@ -494,6 +495,10 @@ plan::Options fused_options(const qse_ctx* ctx, uint32_t n)
     plan::Options opt;
     opt.rb = 4;
     opt.k = tile_qubits_for(ctx, n, 4, 12);
+    // specialised tile kernels on 4096-amplitude tiles hold 32 amplitudes per
+    // thread (128 threads, three CTAs per SM): twice the independent FP64 work
+    // per thread and one layout exchange per five register qubits instead of four
+    if (ctx->jit == 1 && opt.k == 12) opt.rb = 5;
     opt.max_gates = uint32_t(std::max(0, ctx->max_gates_per_pass));
     if (ctx->jit && (opt.max_gates == 0 || opt.max_gates > plan::kJitMaxGates)) opt.max_gates = plan::kJitMaxGates;
     opt.zz_fuse = true;

@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -90,7 +91,7 @@ struct Gen {
     std::ostringstream o;
     std::vector<double> prm;
     uint32_t R, T, NW;
-    int reg[4];
+    int reg[5];
     int thr[16];
     int nthr;
 
@@ -248,7 +249,7 @@ struct Gen {
         o << "  " << ty << " at = " << one;
         for (uint32_t i = 0; i < P.rb; ++i) o << ", ar" << i << " = " << one;
         o << ";\n";
-        for (uint32_t i = P.rb; i < 4; ++i) o << "  " << ty << " ar" << i << " = " << one << "; (void)ar" << i << ";\n";
+        for (uint32_t i = P.rb; i < 5; ++i) o << "  " << ty << " ar" << i << " = " << one << "; (void)ar" << i << ";\n";
     }
 
     // ---- acc_mul: merged diagonal runs ----
@@ -264,9 +265,10 @@ struct Gen {
     struct Item { uint16_t tcond; uint16_t g; };
     struct Fac { std::vector<Item> items; bool hc = false; double ca = 1.0, cb = 0.0; };
     static constexpr uint32_t kMaxTables = 32;
+    static constexpr int kThrChain = 5;   // chain index of the thread accumulator (after ar0..ar4)
     uint32_t max_tables = kMaxTables;   // 0 with precomputed group values (no prologue)
     std::vector<plan::KOp> run_ops;
-    std::vector<Item> chain[5];   // pending accumulator groups: ar0..ar3, at
+    std::vector<Item> chain[kThrChain + 1];   // pending accumulator groups: ar0..ar4, at
     std::ostringstream tabs;      // prologue code building the lane tables
     uint32_t ntab = 0;
     uint32_t nvar = 0;
@@ -369,13 +371,13 @@ struct Gen {
         for (const KOp& op : run_ops) {
             switch (op.kind) {
             case K_ACC_REG: chain[op.p].push_back(Item{op.tcond, op.g}); break;
-            case K_ACC_THR: chain[4].push_back(Item{op.tcond, op.g}); break;
+            case K_ACC_THR: chain[kThrChain].push_back(Item{op.tcond, op.g}); break;
             case K_PHD: fac[op.f].items.push_back(Item{op.tcond, op.g}); break;
             case K_FLUSH_REG: take(op.p, 1 << op.p); break;
             case K_FLUSH_ALL: {
                 for (uint32_t r = 0; r < P.rb; ++r)
                     if ((op.f >> r) & 1) take(int(r), 1 << r);
-                take(4, 0);
+                take(kThrChain, 0);
                 if (!(op.a == 1.0 && op.b == 0.0)) {
                     Fac& f = fac[0];
                     const double a = f.ca * op.a - f.cb * op.b, b = f.ca * op.b + f.cb * op.a;
@@ -598,8 +600,11 @@ struct Gen {
         std::ostringstream src;
         src << kPrelude << "\n";
         src << "struct Prm { double v[" << std::max<size_t>(1, prm.size()) << "]; };\n";
-        // resident CTAs per SM the register budget allows at 128 registers per thread
-        const uint32_t min_blocks = std::max(1u, std::min(8u, 65536u / (T * 128u)));
+        // resident CTAs per SM the register budget allows: 128 registers per
+        // thread, 168 for 32 amplitudes per thread (their 128 registers and the
+        // rest; three CTAs of 128 threads per SM)
+        const uint32_t budget = R >= 32 ? 168u : 128u;
+        const uint32_t min_blocks = std::max(1u, std::min(8u, 65536u / (T * budget)));
         src << "extern \"C\" __global__ void __launch_bounds__(" << T << ", " << min_blocks << ") " << kernel_name() << "("
             << "double2* __restrict__ psi, double2* __restrict__ lam, const TermRec* __restrict__ terms, "
             << "const GroupRec* __restrict__ groups, double* __restrict__ slot_partial, u32* __restrict__ status, "
@@ -979,7 +984,7 @@ struct Gen {
         case K_TRANSPOSE: {
             const LayoutRec& nl = P.layouts[op.g];
             o << "  {\n    const u32 sw = " << slot_expr(nl) << ";\n";
-            uint32_t woff[16];
+            uint32_t woff[32];
             for (uint32_t j = 0; j < R; ++j) woff[j] = slot_off(nl, j);
             set_layout(nl);
             o << "    const u32 sr = " << slot_expr(nl) << ";\n";
@@ -1170,6 +1175,17 @@ std::vector<std::shared_ptr<Kernel>> get_kernels(const std::vector<const Source*
             for (size_t w; (w = next.fetch_add(1)) < todo.size();) bins[w] = compile_to_cubin(srcs[todo[w]]->code, errs[w]);
         });
     for (auto& th : pool) th.join();
+    // QSE_JIT_DUMP=<directory>: every source compiled is also written there
+    // (<entry point>_<hash of the source>.cu), for reading the generated kernels
+    if (const char* dir = std::getenv("QSE_JIT_DUMP"); dir && *dir)
+        for (size_t i : todo) {
+            char name[64];
+            std::snprintf(name, sizeof(name), "_%016zx.cu", std::hash<std::string>{}(srcs[i]->code));
+            if (FILE* f = std::fopen((std::string(dir) + "/" + srcs[i]->name + name).c_str(), "w")) {
+                std::fwrite(srcs[i]->code.data(), 1, srcs[i]->code.size(), f);
+                std::fclose(f);
+            }
+        }
     std::lock_guard<std::mutex> lk(g_mu);
     for (size_t w = 0; w < todo.size(); ++w) {
         if (bins[w].empty()) fail(QSE_ERR_CUDA, "pass kernel compilation failed: " + errs[w]);

@@ -308,7 +308,7 @@ private:
     uint32_t n_;
     const Options& opt_;
     int loc_[64];
-    int reg_[4] = {0, 0, 0, 0};
+    int reg_[5] = {0, 0, 0, 0, 0};
     int thr_[16];
     int nthr_ = 0;
     double gphase_ = 0.0;

@@ -55,9 +55,9 @@ struct KOp {
 static_assert(sizeof(KOp) == 32, "KOp layout");
 
 struct LayoutRec {
-    uint8_t reg[4];    // tile-local bits held in registers (register index bit i <-> reg[i])
+    uint8_t reg[5];    // tile-local bits held in registers (register index bit i <-> reg[i]; rb <= 5)
     uint8_t nthr;      // number of thread-index bits
-    uint8_t pad[3];
+    uint8_t pad[2];
     uint16_t L[16];    // shared-memory slot image of every tile-local bit (XOR-linear map)
     uint8_t thr[16];   // tile-local bit of thread-index bit t (ascending), t < nthr
 };
@@ -128,7 +128,7 @@ constexpr uint32_t kJitMaxGates = 256;
 
 struct Options {
     uint32_t k = 12;             // tile qubits (clamped to n)
-    uint32_t rb = 4;             // register bits per thread
+    uint32_t rb = 4;             // register bits per thread (at most 5; the interpreter kernel takes 3 or 4)
     uint32_t max_gates = 0;      // 0 = no cap on non-diagonal gates per pass
     uint32_t max_terms = 1024;   // diagonal terms per pass (shared-memory group table)
     bool grads = false;          // emit K_GRAD_* for gates with grad >= 0
