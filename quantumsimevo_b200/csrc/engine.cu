@@ -344,6 +344,7 @@ std::shared_ptr<PlanEntry> plan_for(qse_state* st, const std::vector<plan::Gate>
         w.put(prob_out);
         w.put(st->lazy_basis);
         w.put(st->lazy_basis ? st->lazy_umask : 0);
+        w.put(st->lazy_basis ? st->lazy_pmask : 0);
         const char* dbg = std::getenv("QSE_DEBUG_BOUNDS");   // read by jit::generate
         w.s.append(dbg ? dbg : "");
         w.put('\0');
@@ -365,7 +366,8 @@ std::shared_ptr<PlanEntry> plan_for(qse_state* st, const std::vector<plan::Gate>
         const bool basis_in = i == 0 && ns == 1 && st->lazy_basis;
         const bool prob = prob_out && ns == 1 && i + 1 == pl.passes.size();
         e->srcs.push_back(jit::generate(pl.passes[i], ns, basis_in, ctx->jit == 2, st->n >= jit::kPreGroupQubits,
-                                        basis_in ? st->lazy_umask : 0, prob ? lpos : nullptr));
+                                        basis_in ? st->lazy_umask : 0, prob ? lpos : nullptr,
+                                        basis_in ? st->lazy_pmask : 0));
     }
     if (st->n >= kJitAlwaysQubits || jit::count_uncached(e->srcs) <= kJitMaxNewKernels) {
         plan_cache_insert(ctx, e);
@@ -532,6 +534,7 @@ uint64_t run_fused(qse_state* st, const std::vector<plan::Gate>& gates, bool pro
     if (!up.args.empty()) {   // the first pass wrote every amplitude
         st->lazy_basis = false;
         st->lazy_umask = 0;
+        st->lazy_pmask = 0;
         st->lazy_src = nullptr;
     }
     for (uint32_t q = 0; q < st->n; ++q) st->perm[q] = pl.perm_final[q];
@@ -638,7 +641,7 @@ qse_state* compact_state(qse_ctx* ctx, uint32_t m)
         auto* cs = new qse_state;
         cs->ctx = ctx;
         cs->n = kCompactMaxQubits;
-        if (cudaMalloc(&cs->amp, cs->size() * 16) != cudaSuccess) {
+        if (cudaMalloc(&cs->amp, (cs->size() + 128) * 16) != cudaSuccess) {   // + the product qubits' table
             cudaGetLastError();
             delete cs;
             fail(QSE_ERR_OOM, "device allocation of the compact state failed");
@@ -650,6 +653,107 @@ qse_state* compact_state(qse_ctx* ctx, uint32_t m)
     for (uint32_t q = 0; q < 64; ++q) cs->perm[q] = q;
     cs->touch();
     return cs;
+}
+
+// logical qubits a gate involves
+uint64_t gate_support(const plan::Gate& g)
+{
+    auto b = [](uint32_t q) { return uint64_t(1) << q; };
+    switch (g.type) {
+    case QSE_GATE_IDENTITY: return 0;
+    case QSE_GATE_CNOT: case QSE_GATE_CPHASE: case QSE_GATE_SWAP: return b(g.t) | b(g.c);
+    case QSE_GATE_MCPHASE: return b(g.t) | g.cmask;
+    default: return b(g.t);
+    }
+}
+
+bool one_qubit_gate(int type)
+{
+    switch (type) {
+    case QSE_GATE_H: case QSE_GATE_X: case QSE_GATE_Y: case QSE_GATE_Z: case QSE_GATE_PHASE:
+    case QSE_GATE_RX: case QSE_GATE_RY: case QSE_GATE_RZ: case QSE_GATE_2X2:
+        return true;
+    default: return false;
+    }
+}
+
+// v <- (matrix of g) v for a one-qubit gate; v = (re, im) of the qubit's |0>
+// and |1> amplitudes (the matrices of the pass kernels' ops and of apply_plain)
+void apply_one_qubit(const plan::Gate& g, double* v)
+{
+    const double a0 = v[0], b0 = v[1], a1 = v[2], b1 = v[3];
+    auto set = [&](double r0, double i0, double r1, double i1) {
+        v[0] = r0;
+        v[1] = i0;
+        v[2] = r1;
+        v[3] = i1;
+    };
+    const double c = std::cos(g.theta / 2.0), s = std::sin(g.theta / 2.0);
+    switch (g.type) {
+    case QSE_GATE_H: {
+        const double h = 0.70710678118654752440;   // 1/sqrt(2)
+        set(h * (a0 + a1), h * (b0 + b1), h * (a0 - a1), h * (b0 - b1));
+        return;
+    }
+    case QSE_GATE_X: set(a1, b1, a0, b0); return;
+    case QSE_GATE_Y: set(b1, -a1, -b0, a0); return;   // [[0, -i], [i, 0]]
+    case QSE_GATE_Z: set(a0, b0, -a1, -b1); return;
+    case QSE_GATE_PHASE: {
+        const double pc = std::cos(g.theta), ps = std::sin(g.theta);
+        set(a0, b0, a1 * pc - b1 * ps, a1 * ps + b1 * pc);
+        return;
+    }
+    case QSE_GATE_RX: set(c * a0 + s * b1, c * b0 - s * a1, s * b0 + c * a1, c * b1 - s * a0); return;   // [[c, -is], [-is, c]]
+    case QSE_GATE_RY: set(c * a0 - s * a1, c * b0 - s * b1, s * a0 + c * a1, s * b0 + c * b1); return;   // [[c, -s], [s, c]]
+    case QSE_GATE_RZ: set(a0 * c + b0 * s, b0 * c - a0 * s, a1 * c - b1 * s, a1 * s + b1 * c); return;   // diag(e^-i/2, e^i/2)
+    case QSE_GATE_2X2: {
+        const double* m = g.m;
+        set(m[0] * a0 - m[1] * b0 + m[2] * a1 - m[3] * b1, m[0] * b0 + m[1] * a0 + m[2] * b1 + m[3] * a1,
+            m[4] * a0 - m[5] * b0 + m[6] * a1 - m[7] * b1, m[4] * b0 + m[5] * a0 + m[6] * b1 + m[7] * a1);
+        return;
+    }
+    default: fail(QSE_ERR_INVALID, "internal: not a one-qubit gate");
+    }
+}
+
+// Product qubits: a qubit outside the compact state (mask `compact`) whose
+// first gates after the prefix act on it alone stays in a single-qubit state
+// through them (its basis bit from lbits, then those gates).  For every such
+// qubit whose leading gates include a non-diagonal one, the gates leave `rest`
+// and its two amplitudes go to phi[q] (re0, im0, re1, im1); returns the mask of
+// those qubits.  The first pass over the full state multiplies them into its
+// input, instead of applying the gates to every amplitude.
+uint64_t absorb_product_qubits(std::vector<plan::Gate>& rest, uint64_t compact, uint64_t lbits, double (*phi)[4])
+{
+    uint64_t blocked = compact, nondiag = 0;
+    std::vector<char> lead(rest.size(), 0);
+    for (size_t i = 0; i < rest.size(); ++i) {
+        const plan::Gate& g = rest[i];
+        if (one_qubit_gate(g.type) && !((blocked >> g.t) & 1)) {
+            lead[i] = 1;
+            nondiag |= gate_nondiag(g);
+            continue;
+        }
+        blocked |= gate_support(g);
+    }
+    const uint64_t pq = nondiag;   // a run of phases alone stays a basis qubit with its phases in the plan
+    if (!pq) return 0;
+    for (uint64_t s = pq; s; s &= s - 1) {
+        const uint32_t q = uint32_t(__builtin_ctzll(s));
+        const bool one = (lbits >> q) & 1;
+        phi[q][0] = one ? 0.0 : 1.0;
+        phi[q][1] = 0.0;
+        phi[q][2] = one ? 1.0 : 0.0;
+        phi[q][3] = 0.0;
+    }
+    std::vector<plan::Gate> kept;
+    kept.reserve(rest.size());
+    for (size_t i = 0; i < rest.size(); ++i) {
+        if (lead[i] && ((pq >> rest[i].t) & 1)) apply_one_qubit(rest[i], phi[rest[i].t]);
+        else kept.push_back(rest[i]);
+    }
+    rest.swap(kept);
+    return pq;
 }
 
 // Runs the longest prefix of the plan's passes (at least two) whose gates
@@ -732,6 +836,8 @@ bool compact_prefix(qse_state* st, const std::vector<plan::Gate>& gates_in, std:
     rest.clear();
     for (size_t g = 0; g < gates.size(); ++g)
         if (!in_prefix[g]) rest.push_back(gates[g]);
+    double phi[64][4];
+    const uint64_t pq = absorb_product_qubits(rest, uK, lbits, phi);
     // the prefix on the compact state (its passes are not the full state's:
     // they stay out of the pass timings)
     qse_state* cs = compact_state(ctx, m);
@@ -753,7 +859,24 @@ bool compact_prefix(qse_state* st, const std::vector<plan::Gate>& gates_in, std:
         throw;
     }
     ctx->time_passes = timing;
+    // the product qubits' amplitudes after the compact ones, in ascending
+    // physical position
+    uint64_t pmask = 0;
+    for (uint32_t q = 0; q < st->n; ++q)
+        if ((pq >> q) & 1) pmask |= uint64_t(1) << st->perm[q];
+    if (pmask) {
+        std::vector<double> tab;
+        for (uint64_t s = pmask; s; s &= s - 1) {
+            const uint32_t p = uint32_t(__builtin_ctzll(s));
+            uint32_t q = 0;
+            while (st->perm[q] != p) ++q;
+            tab.insert(tab.end(), phi[q], phi[q] + 4);
+        }
+        QSE_CUDA(cudaMemcpyAsync(cs->amp + 2 * (size_t(1) << m), tab.data(), tab.size() * 8, cudaMemcpyHostToDevice,
+                                 ctx->stream));
+    }
     st->lazy_umask = umask;
+    st->lazy_pmask = pmask;
     st->lazy_src = cs->amp;
     return true;
 }

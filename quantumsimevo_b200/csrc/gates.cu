@@ -440,6 +440,7 @@ void mark_basis(qse_state* st, uint64_t phys_index)
     st->lazy_basis = true;
     st->lazy_index = phys_index;
     st->lazy_umask = 0;
+    st->lazy_pmask = 0;
     st->lazy_src = nullptr;
     st->touch();
 }
@@ -449,6 +450,7 @@ void write_basis_state(qse_state* st, uint64_t phys_index)
 {
     st->lazy_basis = false;
     st->lazy_umask = 0;
+    st->lazy_pmask = 0;
     st->lazy_src = nullptr;
     st->touch();
     QSE_CUDA(cudaMemsetAsync(st->amp, 0, st->size() * 16, st->ctx->stream));
@@ -470,20 +472,49 @@ __global__ void __launch_bounds__(kBlock) k_expand_compact(double2* __restrict__
     }
 }
 
+// out[x] for every x < size: 0 unless x's bits outside umask | pmask equal
+// fixed's, else src[pext(x, umask)] times, for the i-th qubit of pmask
+// (ascending), src[count + 2i + its bit of x]
+__global__ void __launch_bounds__(kBlock) k_expand_product(double2* __restrict__ out, const double2* __restrict__ src,
+                                                          uint64_t size, uint64_t count, uint64_t umask,
+                                                          uint64_t pmask, uint64_t fixed)
+{
+    const uint64_t zmask = (size - 1) & ~(umask | pmask);
+    for (uint64_t x = blockIdx.x * uint64_t(kBlock) + threadIdx.x; x < size; x += uint64_t(gridDim.x) * kBlock) {
+        if ((x ^ fixed) & zmask) {
+            out[x] = make_double2(0.0, 0.0);
+            continue;
+        }
+        uint64_t c = 0, r = 0;
+        for (uint64_t m = umask; m; m &= m - 1, ++r) c |= ((x >> (__ffsll(static_cast<long long>(m)) - 1)) & 1) << r;
+        double2 v = src[c];
+        uint64_t i = 0;
+        for (uint64_t m = pmask; m; m &= m - 1, ++i)
+            v = cmul(v, src[count + 2 * i + ((x >> (__ffsll(static_cast<long long>(m)) - 1)) & 1)]);
+        out[x] = v;
+    }
+}
+
 // the compact form of a lazy state written out: zeros, then the compact
-// amplitudes at their places
+// amplitudes at their places (with product qubits: every amplitude)
 void write_compact_state(qse_state* st)
 {
-    const uint64_t umask = st->lazy_umask, fixed = st->lazy_index & ~umask;
+    const uint64_t umask = st->lazy_umask, pmask = st->lazy_pmask, fixed = st->lazy_index & ~umask;
     const double2* src = static_cast<const double2*>(st->lazy_src);
     st->lazy_basis = false;
     st->lazy_umask = 0;
+    st->lazy_pmask = 0;
     st->lazy_src = nullptr;
     st->touch();
-    QSE_CUDA(cudaMemsetAsync(st->amp, 0, st->size() * 16, st->ctx->stream));
     const uint64_t count = uint64_t(1) << __builtin_popcountll(umask);
-    k_expand_compact<<<grid_full(count), kBlock, 0, st->ctx->stream>>>(reinterpret_cast<double2*>(st->amp), src, count,
-                                                                       umask, fixed);
+    if (pmask) {
+        k_expand_product<<<grid_full(st->size()), kBlock, 0, st->ctx->stream>>>(
+            reinterpret_cast<double2*>(st->amp), src, st->size(), count, umask, pmask, fixed);
+    } else {
+        QSE_CUDA(cudaMemsetAsync(st->amp, 0, st->size() * 16, st->ctx->stream));
+        k_expand_compact<<<grid_full(count), kBlock, 0, st->ctx->stream>>>(reinterpret_cast<double2*>(st->amp), src,
+                                                                           count, umask, fixed);
+    }
     QSE_CUDA(cudaGetLastError());
     count_launch(st->ctx);
 }

@@ -101,6 +101,11 @@ struct Gen {
     // (lam, 2^popcount(umask) amplitudes indexed by those bits in ascending
     // order); the other qubits hold the bits of bi.  0: the plain basis state
     uint64_t umask = 0;
+    // with umask: product qubits (their amplitude pairs after the compact
+    // state's) and whether any of them sits on a register bit (the pass then
+    // builds the registers' factors in shared memory, pfs)
+    uint64_t pmask = 0;
+    bool preg = false;
     // probability side output (forward passes): logical position of every
     // physical qubit after this pass; empty = none (emit_prob)
     std::vector<uint8_t> lpos;
@@ -110,6 +115,16 @@ struct Gen {
     // the array's size; one outside records 8 in *status and is skipped
     bool dbg = false;
     std::string nstr() const { return hex(uint64_t(1) << (P.k + uint32_t(__builtin_popcountll(P.outer_mask)))); }
+    // index in lam of product qubit q's |0> amplitude, and the size of lam with the product table
+    std::string ph_index(uint32_t q) const
+    {
+        const uint64_t below = uint64_t(__builtin_popcountll(pmask & ((uint64_t(1) << q) - 1)));
+        return hex((uint64_t(1) << __builtin_popcountll(umask)) + 2 * below);
+    }
+    std::string ph_size() const
+    {
+        return hex((uint64_t(1) << __builtin_popcountll(umask)) + 2 * uint64_t(__builtin_popcountll(pmask)));
+    }
     // array[idx] as an operand (a zero amplitude when out of range in debug mode)
     std::string ld(const std::string& arr, const std::string& idx, const std::string& size) const
     {
@@ -505,7 +520,7 @@ struct Gen {
             basis_slot = int(push(0.0));
             o << "  const u64 bi = (u64)P.v[" << basis_slot << "]; (void)bi;\n";
             const uint32_t lt = uint32_t(__builtin_ctz(T));
-            const uint64_t zmask = P.outer_mask & ~umask;
+            const uint64_t zmask = P.outer_mask & ~umask & ~pmask;
             if (zmask) {
                 o << "  if (((ob ^ bi) & " << hex(zmask) << ") != 0ull) {\n    const u64 gz = ob";
                 for (uint32_t b = 0; b < lt; ++b)
@@ -552,7 +567,7 @@ struct Gen {
             }
             uint64_t tmask = 0;
             for (uint32_t b = 0; b < P.k; ++b) tmask |= uint64_t(1) << P.tile_phys[b];
-            const uint64_t tz = tmask & ~umask;
+            const uint64_t tz = tmask & ~umask & ~pmask;
             for (uint32_t j = 0; j < R; ++j) {
                 uint64_t coff = 0;
                 for (uint32_t i = 0; i < P.rb; ++i)
@@ -565,6 +580,21 @@ struct Gen {
                 o << ld("lam", "cb + " + hex(coff), hex(uint64_t(1) << __builtin_popcountll(umask)));
                 if (tz) o << " : make_double2(0.0, 0.0)";
                 o << ";\n";
+            }
+            if (pmask) {
+                // product qubits on outer and thread bits: one factor per thread
+                o << "  double2 pf = make_double2(1.0, 0.0);\n";
+                for (uint32_t q = 0; q < 64; ++q)
+                    if ((P.outer_mask >> q) & (pmask >> q) & 1)
+                        o << "  pf = cmul(pf, " << ld("lam", ph_index(q) + " + ((ob >> " + std::to_string(q) + ") & 1ull)", ph_size())
+                          << ");\n";
+                for (int t = 0; t < nthr; ++t) {
+                    const uint32_t q = P.tile_phys[thr[t]];
+                    if ((pmask >> q) & 1)
+                        o << "  pf = cmul(pf, "
+                          << ld("lam", ph_index(q) + " + (u64)((tid >> " + std::to_string(t) + ") & 1u)", ph_size()) << ");\n";
+                }
+                for (uint32_t i = 0; i < P.rb; ++i) preg |= ((pmask >> P.tile_phys[reg[i]]) & 1) != 0;
             }
         }
         // prologue: per-CTA diagonal group values, then the lane tables
@@ -591,10 +621,36 @@ struct Gen {
         }
         if (ntab) o << "  __syncthreads();\n" << tabs.str();
         if (ns == 2 && nslots) o << "  for (u32 i = tid; i < " << nslots * NW << "u; i += " << T << "u) wp[i] = 0.0;\n";
+        if (preg) {
+            // product qubits on register bits: the factor of every register index
+            o << "  double2* pfs = tb + " << 32 * ntab << ";\n"
+              << "  for (u32 j = tid; j < " << R << "u; j += " << T << "u) {\n    double2 f = make_double2(1.0, 0.0);\n";
+            for (uint32_t i = 0; i < P.rb; ++i) {
+                const uint32_t q = P.tile_phys[reg[i]];
+                if ((pmask >> q) & 1)
+                    o << "    f = cmul(f, " << ld("lam", ph_index(q) + " + (u64)((j >> " + std::to_string(i) + ") & 1u)", ph_size())
+                      << ");\n";
+            }
+            o << "    pfs[j] = f;\n  }\n";
+        }
         o << "  __syncthreads();\n";
         if (zero_in && !umask)
             for (uint32_t j = 0; j < R; ++j)
                 o << "  a0[" << j << "] = make_double2((gb | " << hex(reg_off(j)) << ") == bi ? 1.0 : 0.0, 0.0);\n";
+        if (pmask && !preg) {
+            for (uint32_t j = 0; j < R; ++j) o << "  a0[" << j << "] = cmul(a0[" << j << "], pf);\n";
+        } else if (preg) {
+            bool all = true;   // every register bit a product qubit: one input value per thread
+            for (uint32_t i = 0; i < P.rb; ++i) all = all && ((pmask >> P.tile_phys[reg[i]]) & 1);
+            if (all) {
+                o << "  { const double2 pv = cmul(a0[0], pf);";
+                for (uint32_t j = 0; j < R; ++j) o << " a0[" << j << "] = cmul(pv, pfs[" << j << "]);";
+                o << " }\n";
+            } else {
+                for (uint32_t j = 0; j < R; ++j)
+                    o << "  a0[" << j << "] = cmul(a0[" << j << "], cmul(pf, pfs[" << j << "]));\n";
+            }
+        }
         std::swap(o, head);
 
         std::ostringstream src;
@@ -1101,7 +1157,7 @@ static bool streamable(const plan::PassProgram& p, int nstates, bool basis_input
 }
 
 Source generate(const plan::PassProgram& p, int nstates, bool basis_input, bool streamed, bool precomputed_groups,
-                uint64_t compact_mask, const uint8_t* prob_lpos)
+                uint64_t compact_mask, const uint8_t* prob_lpos, uint64_t product_mask)
 {
     const char* dbg_env = std::getenv("QSE_DEBUG_BOUNDS");
     const bool dbg = dbg_env && *dbg_env && std::strcmp(dbg_env, "0") != 0;
@@ -1118,9 +1174,10 @@ Source generate(const plan::PassProgram& p, int nstates, bool basis_input, bool 
         }
     }
     Gen g(p, nstates, basis_input, precomputed_groups, compact_mask);
+    g.pmask = g.umask ? product_mask : 0;
     g.dbg = dbg;
     // (not with a tile that stores zeros and returns early: a basis input with outer bits)
-    if (prob_lpos && nstates == 1 && !(g.zero_in && (p.outer_mask & ~g.umask) != 0))
+    if (prob_lpos && nstates == 1 && !(g.zero_in && (p.outer_mask & ~g.umask & ~g.pmask) != 0))
         g.lpos.assign(prob_lpos, prob_lpos + 64);
     Source s;
     s.code = g.run();
@@ -1133,7 +1190,7 @@ Source generate(const plan::PassProgram& p, int nstates, bool basis_input, bool 
     s.ngroups = uint32_t(p.groups.size());
     s.threads = g.T;
     s.smem = (size_t(1) << p.k) * 16 + p.groups.size() * 16 + size_t(g.ntab) * 32 * 16 +
-             (nstates == 2 ? p.slot_src.size() * g.NW * 8 : 0);
+             (nstates == 2 ? p.slot_src.size() * g.NW * 8 : 0) + (g.preg ? size_t(g.R) * 16 : 0);
     return s;
 }
 

@@ -63,8 +63,12 @@ size_t compile_only(const Source& s);
 // amplitudes it stores in logical order and their 4096-block sums (passed as
 // `slot_partial` at launch: 2^n doubles, then 2^n / 4096 sums, zeroed before);
 // prob_lpos[q] = logical position of physical qubit q after the pass
+// product_mask (with compact_mask): physical qubits outside the compact state
+// that hold a single-qubit state each, whose two amplitudes (the i-th lowest
+// qubit's at lam[2^popcount(compact_mask) + 2i + bit]) multiply the input
 Source generate(const plan::PassProgram& p, int nstates, bool basis_input = false, bool streamed = false,
-                bool precomputed_groups = false, uint64_t compact_mask = 0, const uint8_t* prob_lpos = nullptr);
+                bool precomputed_groups = false, uint64_t compact_mask = 0, const uint8_t* prob_lpos = nullptr,
+                uint64_t product_mask = 0);
 // distinct sources among srcs that are not compiled yet
 size_t count_uncached(const std::vector<Source>& srcs);
 // compiled kernels for every source (cached by source text; missing ones are compiled in parallel)

@@ -99,8 +99,12 @@ struct qse_state {
                                  // materialize() first (reset: |0..0>; measure: the outcome)
     // with lazy_basis, inside one execute: the state is a compact state on the
     // physical qubits of lazy_umask (lazy_src, indexed by those bits in
-    // ascending order) times the basis bits of lazy_index on the other qubits
+    // ascending order) times, on the qubits of lazy_pmask, one single-qubit
+    // state each (product qubits: the 2 amplitudes of the i-th lowest at
+    // lazy_src[2^popcount(lazy_umask) + 2i + bit]) times the basis bits of
+    // lazy_index on the other qubits
     uint64_t lazy_umask = 0;
+    uint64_t lazy_pmask = 0;
     const void* lazy_src = nullptr;
     // probabilities written by the last pass of an execute (cdf buffer, see
     // prob_buffer_bytes) are current while prob_version == version.  prob_hint:
