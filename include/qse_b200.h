@@ -286,9 +286,8 @@ QSE_API int qse_expectation(qse_state* st, const qse_observable* obs, double* va
  * share that array, so calls that run at the same time race: calls from
  * several host threads (on one context or several) and calls whose GPU work
  * overlaps.  The call is synchronous (it returns once the value is on the
- * host).  The first call on a device looks up the array's address and should
- * come before any stream capture.  No counterpart in the reference (it has
- * no observables). */
+ * host), so it cannot be made during a stream capture.  No counterpart in the
+ * reference (it has no observables). */
 QSE_API int qse_expectation_noalloc(qse_state* st, const qse_observable* obs, double* value);
 /* Runs ops from |0..0> into st, then the adjoint sweep: grad[p] = d<O>/d params[p].
  * Parameterised types: RX, RY, RZ, PHASE, CPHASE, MCPHASE. */

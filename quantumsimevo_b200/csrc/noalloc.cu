@@ -19,10 +19,11 @@
 //     it: calls from several host threads (on one context or several), and
 //     calls whose GPU work overlaps (other streams, other contexts);
 //   - the call is synchronous: it returns after its result has reached the
-//     host (it waits on the context's stream);
+//     host (it waits on the context's stream), so it cannot be made while the
+//     context's stream is being captured into a graph;
 //   - the first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (the host-side name of a __device__ array is not a
-//     device address); make that first call before any stream capture.
+//     device address).
 #include <cuda_runtime.h>
 
 #include <mutex>
