@@ -273,12 +273,17 @@ Uploaded upload_plan(qse_ctx* ctx, const plan::Plan& pl, bool term_phases = fals
 // sincos.  Other groups keep the plain sum of their angles.  A CTA handles
 // kGvTiles consecutive tiles: their outer bits once into shared memory, then
 // its threads walk the rows' elements in address order (coalesced stores).
+// For the two tables of a split pass (jit::Source::gv_lo) the "tiles" are the
+// values of one part of the outer qubits (outer_mask = that part); a term
+// conditioned on the other part never holds there, and skip_unconditioned
+// leaves the terms without a condition to the other table.
 constexpr uint32_t kGvTiles = 32;
 
 __global__ void __launch_bounds__(256) k_group_values(const plan::TermRec* __restrict__ terms,
                                                       const double2* __restrict__ texp,
                                                       const plan::GroupRec* __restrict__ groups, uint32_t ng,
-                                                      uint64_t outer_mask, uint64_t ntiles, double2* __restrict__ out)
+                                                      uint64_t outer_mask, uint64_t ntiles, double2* __restrict__ out,
+                                                      bool skip_unconditioned)
 {
     __shared__ uint64_t s_ob[kGvTiles];
     const uint64_t t0 = uint64_t(blockIdx.x) * kGvTiles;
@@ -301,16 +306,18 @@ __global__ void __launch_bounds__(256) k_group_values(const plan::TermRec* __res
         double2 v;
         if (gr.direct) {
             v = make_double2(1.0, 0.0);
-            for (uint32_t k = 0; k < gr.count; ++k)
-                if ((ob & terms[gr.first + k].ocond) == terms[gr.first + k].ocond) {
+            for (uint32_t k = 0; k < gr.count; ++k) {
+                const uint64_t oc = terms[gr.first + k].ocond;
+                if ((ob & oc) == oc && (oc || !skip_unconditioned)) {
                     const double2 f = texp[gr.first + k];
                     v = make_double2(v.x * f.x - v.y * f.y, v.x * f.y + v.y * f.x);
                 }
+            }
         } else {
             double th = 0.0;
             for (uint32_t k = 0; k < gr.count; ++k) {
                 const plan::TermRec t = terms[gr.first + k];
-                if ((ob & t.ocond) == t.ocond) th += t.theta;
+                if ((ob & t.ocond) == t.ocond && (t.ocond || !skip_unconditioned)) th += t.theta;
             }
             v = make_double2(th, 0.0);
         }
@@ -427,15 +434,26 @@ struct PassRunner {
         }
         const void* gvt = nullptr;
         if (srcs[i].pre_gv) {
-            const uint64_t ntiles = uint64_t(1) << (st->n - kq[i]);
-            const uint64_t cnt = ntiles * srcs[i].ngroups;
-            ctx->gv_buf.reserve(cnt * sizeof(double2));
-            const uint64_t blocks = (ntiles + kGvTiles - 1) / kGvTiles;
-            k_group_values<<<unsigned(blocks), 256, 0, ctx->stream>>>(a.terms, up.texp[i], a.groups, srcs[i].ngroups,
-                                                                     a.outer_mask, ntiles,
-                                                                     static_cast<double2*>(ctx->gv_buf.ptr));
-            QSE_CUDA(cudaGetLastError());
-            count_launch(ctx);
+            // one table of every tile's row, or (gv_lo) a table for each part of the outer qubits
+            const uint32_t nob = st->n - kq[i], lo = srcs[i].gv_lo;
+            uint64_t lomask = 0, m = a.outer_mask;
+            for (uint32_t b = 0; b < lo; ++b, m &= m - 1) lomask |= m & (~m + 1);
+            struct Part { uint64_t mask, ntiles; bool skip; };
+            const Part parts[2] = {{lo ? lomask : a.outer_mask, uint64_t(1) << (lo ? lo : nob), false},
+                                   {a.outer_mask & ~lomask, uint64_t(1) << (nob - lo), true}};
+            const int nparts = lo ? 2 : 1;
+            const uint64_t ng = srcs[i].ngroups;
+            ctx->gv_buf.reserve((parts[0].ntiles + (lo ? parts[1].ntiles : 0)) * ng * sizeof(double2));
+            double2* out = static_cast<double2*>(ctx->gv_buf.ptr);
+            for (int p = 0; p < nparts; ++p) {
+                const uint64_t blocks = (parts[p].ntiles + kGvTiles - 1) / kGvTiles;
+                k_group_values<<<unsigned(blocks), 256, 0, ctx->stream>>>(a.terms, up.texp[i], a.groups, uint32_t(ng),
+                                                                         parts[p].mask, parts[p].ntiles, out,
+                                                                         parts[p].skip);
+                QSE_CUDA(cudaGetLastError());
+                count_launch(ctx);
+                out += parts[p].ntiles * ng;
+            }
             gvt = ctx->gv_buf.ptr;
         }
         cudaEvent_t stop = tile::pass_timer_begin(ctx);

@@ -152,6 +152,7 @@ struct Gen {
     // of ng values per tile): the prologue copies them instead of summing terms
     // and calling sincos per group
     bool pre_gv = false;
+    uint32_t gv_lo = 0;   // pre_gv from two tables split at this many low CTA-index bits (Source::gv_lo)
 
     Gen(const plan::PassProgram& p, int nstates, bool zero_input, bool precomputed_groups = false,
         uint64_t compact_mask = 0)
@@ -161,6 +162,14 @@ struct Gen {
         R = 1u << P.rb;
         T = 1u << (P.k - P.rb);
         NW = std::max(1u, T / 32);
+        const uint32_t nob = uint32_t(__builtin_popcountll(P.outer_mask));
+        if (pre_gv && nob >= 2) {
+            uint64_t lo = 0, m = P.outer_mask;
+            for (uint32_t i = 0; i < nob / 2; ++i, m &= m - 1) lo |= m & (~m + 1);
+            bool split = true;
+            for (const plan::TermRec& t : P.terms) split = split && ((t.ocond & lo) == 0 || (t.ocond & ~lo) == 0);
+            if (split) gv_lo = nob / 2;
+        }
     }
 
     void set_layout(const plan::LayoutRec& L)
@@ -598,7 +607,27 @@ struct Gen {
             }
         }
         // prologue: per-CTA diagonal group values, then the lane tables
-        if (ng && pre_gv) {
+        if (ng && pre_gv && gv_lo) {
+            const uint32_t nob = uint32_t(__builtin_popcountll(P.outer_mask));
+            const uint64_t rows_lo = uint64_t(1) << gv_lo;
+            const std::string total = hex((rows_lo + (uint64_t(1) << (nob - gv_lo))) * ng);
+            o << "  for (u32 g = tid; g < " << ng << "u; g += " << T << "u) {\n"
+              << "    const double2 l = "
+              << ld("gvt", "(u64)(blockIdx.x & " + hex(rows_lo - 1) + ") * " + std::to_string(ng) + "u + g", total) << ";\n"
+              << "    const double2 h = "
+              << ld("gvt", hex(rows_lo * ng) + " + (u64)(blockIdx.x >> " + std::to_string(gv_lo) + ") * " +
+                               std::to_string(ng) + "u + g", total)
+              << ";\n";
+            // the groups' kinds are known here: no load of the group records
+            bool all_direct = true, none_direct = true;
+            for (const plan::GroupRec& gr : P.groups) {
+                all_direct = all_direct && gr.direct;
+                none_direct = none_direct && !gr.direct;
+            }
+            if (all_direct) o << "    gv[g] = cmul(l, h);\n  }\n";
+            else if (none_direct) o << "    gv[g] = make_double2(l.x + h.x, 0.0);\n  }\n";
+            else o << "    gv[g] = groups[g].direct ? cmul(l, h) : make_double2(l.x + h.x, 0.0);\n  }\n";
+        } else if (ng && pre_gv) {
             o << "  for (u32 g = tid; g < " << ng << "u; g += " << T << "u) gv[g] = "
               << ld("gvt", "(u64)blockIdx.x * " + std::to_string(ng) + "u + g", "(u64)gridDim.x * " + std::to_string(ng) + "u")
               << ";\n";
@@ -1184,6 +1213,7 @@ Source generate(const plan::PassProgram& p, int nstates, bool basis_input, bool 
     s.prm = std::move(g.prm);
     s.basis_slot = g.basis_slot;
     s.pre_gv = g.pre_gv;
+    s.gv_lo = g.gv_lo;
     s.name = g.kernel_name();
     s.prob = !g.lpos.empty();
     s.prob_bsum = g.prob_bsum;

@@ -26,6 +26,12 @@ struct Source {
     bool streamed = false;    // persistent streamed kernel (grid = SM count) instead of one CTA per tile
     bool pre_gv = false;      // the per-CTA group values are read from a precomputed table (gvt)
     uint32_t ngroups = 0;     // diagonal groups of the pass (the table's row length)
+    // pre_gv with gv_lo > 0: every term's outer condition lies in the lowest
+    // gv_lo outer qubits or in the others, so the table is two tables: one row
+    // per value of the low gv_lo CTA-index bits, then one per value of the
+    // other bits (terms without a condition in the first only); a CTA's value
+    // is the product (direct groups) or the sum (angle groups) of its two rows'
+    uint32_t gv_lo = 0;
 };
 
 // States of at least this many qubits run their passes with the group values
