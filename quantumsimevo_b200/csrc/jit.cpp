@@ -618,15 +618,19 @@ struct Gen {
               << ld("gvt", hex(rows_lo * ng) + " + (u64)(blockIdx.x >> " + std::to_string(gv_lo) + ") * " +
                                std::to_string(ng) + "u + g", total)
               << ";\n";
-            // the groups' kinds are known here: no load of the group records
+            // the groups' kinds are known here: no load of the group records.  The
+            // product's roundings are written out (no contraction left to the
+            // compiler), so the debug mode's kernel gives the same bits
             bool all_direct = true, none_direct = true;
             for (const plan::GroupRec& gr : P.groups) {
                 all_direct = all_direct && gr.direct;
                 none_direct = none_direct && !gr.direct;
             }
-            if (all_direct) o << "    gv[g] = cmul(l, h);\n  }\n";
-            else if (none_direct) o << "    gv[g] = make_double2(l.x + h.x, 0.0);\n  }\n";
-            else o << "    gv[g] = groups[g].direct ? cmul(l, h) : make_double2(l.x + h.x, 0.0);\n  }\n";
+            const std::string prod = "make_double2(__fma_rn(l.x, h.x, -__dmul_rn(l.y, h.y)), __fma_rn(l.x, h.y, __dmul_rn(l.y, h.x)))";
+            const std::string sum = "make_double2(__dadd_rn(l.x, h.x), 0.0)";
+            if (all_direct) o << "    gv[g] = " << prod << ";\n  }\n";
+            else if (none_direct) o << "    gv[g] = " << sum << ";\n  }\n";
+            else o << "    gv[g] = groups[g].direct ? " << prod << " : " << sum << ";\n  }\n";
         } else if (ng && pre_gv) {
             o << "  for (u32 g = tid; g < " << ng << "u; g += " << T << "u) gv[g] = "
               << ld("gvt", "(u64)blockIdx.x * " + std::to_string(ng) + "u + g", "(u64)gridDim.x * " + std::to_string(ng) + "u")
